@@ -1,0 +1,246 @@
+"""clwilson_b200 -- B200-native Wilson-prime search engine.
+
+Python host bindings over the C ABI of ``libwilson.so`` (include/wilson.h).
+The computation runs only in the CUDA kernels of that library; importing this
+package without the built library raises, and there is no CPU fallback.
+
+Mirrors the reference program's surface (mfl0p/CLWilson):
+  * ``search(pmin, pmax)``      one run of cl_wilson() (cl_wilson.cpp:1442-1974):
+                                result lines and checksum
+  * ``rows(pmin, pmax)``        per-prime residues and quotients
+  * ``batch(ranges)``           many ranges in one device pass
+  * ``write_results(...)``      results.txt in the reference's byte format
+                                (cl_wilson.cpp:657-688, 1093-1143)
+  * ``parse_uint64``            the CLI number parser (putil.c:34-116)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libwilson.so")
+
+WL_MAXP = 4611686018427387903
+WL_MAX_WIDTH = 10_000_000
+ERRORS = {
+    -1: "invalid argument or range", -2: "CUDA error", -3: "there are no primes to test in this range!",
+    -4: "configuration not supported by this build", -5: "Wilson quotient check failed",
+    -6: "representation a, c or u not found", -7: "result buffer too small", -8: "device allocation failed",
+}
+
+
+class WilsonError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__(f"{what}: {ERRORS.get(code, 'unknown error')} ({code})" if what else ERRORS.get(code, str(code)))
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_uint64), ("value", ctypes.c_int32), ("pad", ctypes.c_uint32)]
+
+
+class _Row(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_uint64), ("s0", ctypes.c_uint64), ("s1", ctypes.c_uint64),
+                ("rem", ctypes.c_uint64), ("quot", ctypes.c_uint64), ("type", ctypes.c_uint32),
+                ("status", ctypes.c_uint32)]
+
+
+class _Range(ctypes.Structure):
+    _fields_ = [("pmin", ctypes.c_uint64), ("pmax", ctypes.c_uint64)]
+
+
+class _RangeResult(ctypes.Structure):
+    _fields_ = [("tested", ctypes.c_uint64), ("checksum", ctypes.c_uint64), ("targets", ctypes.c_uint64 * 3),
+                ("results", ctypes.c_uint32), ("status", ctypes.c_uint32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("tested", ctypes.c_uint64), ("per_class", ctypes.c_uint64 * 3), ("targets", ctypes.c_uint64 * 3),
+                ("pi_maxtarget", ctypes.c_uint64), ("cells", ctypes.c_uint64), ("tail_steps", ctypes.c_uint64),
+                ("checksum", ctypes.c_uint64), ("results", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+                ("ms_device", ctypes.c_double), ("ms_primes", ctypes.c_double), ("ms_sieve", ctypes.c_double),
+                ("ms_sweep", ctypes.c_double), ("ms_iterate", ctypes.c_double), ("ms_finish", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
+
+
+ROW_DTYPE = np.dtype([("p", "<u8"), ("s0", "<u8"), ("s1", "<u8"), ("rem", "<u8"), ("quot", "<u8"),
+                      ("type", "<u4"), ("status", "<u4")])
+assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
+
+# exported symbols of include/wilson.h
+SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
+           "wl_batch", "wl_parse_uint64")
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libwilson.so and declare its C signatures.  Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libwilson.so not built ({path}); run `python -m clwilson_b200.build`")
+    L = ctypes.CDLL(path)
+    u64, vp, sz = ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t
+    L.wl_open.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.wl_open.restype = ctypes.c_int
+    L.wl_close.argtypes = [vp]
+    L.wl_close.restype = None
+    L.wl_strerror.argtypes = [ctypes.c_int]
+    L.wl_strerror.restype = ctypes.c_char_p
+    L.wl_stream.argtypes = [vp]
+    L.wl_stream.restype = vp
+    L.wl_check_range.argtypes = [u64, u64]
+    L.wl_check_range.restype = ctypes.c_int
+    L.wl_search.argtypes = [vp, u64, u64, u64, ctypes.POINTER(_Result), sz, ctypes.POINTER(_Stats)]
+    L.wl_search.restype = ctypes.c_int
+    L.wl_rows.argtypes = [vp, u64, u64, u64, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(_Stats)]
+    L.wl_rows.restype = ctypes.c_int
+    L.wl_batch.argtypes = [vp, ctypes.POINTER(_Range), sz, u64, ctypes.POINTER(_RangeResult),
+                           ctypes.POINTER(_Result), sz, ctypes.POINTER(sz), ctypes.POINTER(_Stats)]
+    L.wl_batch.restype = ctypes.c_int
+    L.wl_parse_uint64.argtypes = [ctypes.POINTER(u64), ctypes.c_char_p, u64, u64]
+    L.wl_parse_uint64.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def parse_uint64(text: str, lo: int, hi: int) -> Tuple[int, int]:
+    """(status, value): status 0 ok, -1 cannot parse, -2 out of range (putil.c:34-116)."""
+    L = load_library()
+    v = ctypes.c_uint64(0)
+    rc = L.wl_parse_uint64(ctypes.byref(v), text.encode(), lo, hi)
+    return rc, v.value
+
+
+def check_range(pmin: int, pmax: int) -> int:
+    return load_library().wl_check_range(pmin, pmax)
+
+
+@dataclass
+class Stats:
+    tested: int = 0
+    per_class: Tuple[int, int, int] = (0, 0, 0)
+    targets: Tuple[int, int, int] = (0, 0, 0)
+    pi_maxtarget: int = 0
+    cells: int = 0
+    tail_steps: int = 0
+    checksum: int = 0
+    results: int = 0
+    kernel_launches: int = 0
+    ms_device: float = 0.0
+    ms_primes: float = 0.0
+    ms_sieve: float = 0.0
+    ms_sweep: float = 0.0
+    ms_iterate: float = 0.0
+    ms_finish: float = 0.0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+
+    @classmethod
+    def from_c(cls, s: _Stats) -> "Stats":
+        return cls(s.tested, tuple(s.per_class), tuple(s.targets), s.pi_maxtarget, s.cells, s.tail_steps,
+                   s.checksum, s.results, s.kernel_launches, s.ms_device, s.ms_primes, s.ms_sieve, s.ms_sweep,
+                   s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes)
+
+
+@dataclass
+class SearchResult:
+    results: List[Tuple[int, int]]   # (p, value): value 0 = Wilson prime, else Near-Wilson +-value
+    checksum: int
+    stats: Stats = field(default_factory=Stats)
+
+    def lines(self) -> List[str]:
+        return [result_line(p, v) for p, v in self.results]
+
+
+def result_line(p: int, value: int) -> str:
+    """One results.txt line (cl_wilson.cpp:665-676)."""
+    if value == 0:
+        return f"{p} is a Wilson prime"
+    return f"{p} is a Near-Wilson prime {value:+d}"
+
+
+def write_results(path: str, results: Sequence[Tuple[int, int]], checksum: int, append: bool = False) -> None:
+    """results.txt: the lines in ascending p, then the checksum line
+    (finalizeResults, cl_wilson.cpp:1126-1137)."""
+    with open(path, "a" if append else "w") as f:
+        for p, v in results:
+            f.write(result_line(p, v) + "\n")
+        if results:
+            f.write("%016X\n" % checksum)
+        else:
+            f.write("no results\n%016X\n" % checksum)
+
+
+class Engine:
+    """One context on one GPU (wl_open / wl_close)."""
+
+    def __init__(self, device: int = 0):
+        self._L = load_library()
+        self._ctx = ctypes.c_void_p()
+        rc = self._L.wl_open(device, ctypes.byref(self._ctx))
+        if rc:
+            raise WilsonError(rc, "wl_open")
+
+    def close(self) -> None:
+        if self._ctx:
+            self._L.wl_close(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return self._L.wl_stream(self._ctx) or 0
+
+    def search(self, pmin: int, pmax: int, q_cap: int = 0, cap: int = 1 << 16) -> SearchResult:
+        res = (_Result * cap)()
+        st = _Stats()
+        rc = self._L.wl_search(self._ctx, pmin, pmax, q_cap, res, cap, ctypes.byref(st))
+        if rc:
+            raise WilsonError(rc, "wl_search")
+        out = [(res[i].p, res[i].value) for i in range(min(st.results, cap))]
+        return SearchResult(out, st.checksum, Stats.from_c(st))
+
+    def rows(self, pmin: int, pmax: int, q_cap: int = 0) -> Tuple[np.ndarray, Stats]:
+        n = ctypes.c_size_t(0)
+        st = _Stats()
+        # size the buffer generously: primes in the window are < width/2 + 2
+        cap = (pmax - pmin) // 2 + 2
+        buf = np.zeros(cap, dtype=ROW_DTYPE)
+        rc = self._L.wl_rows(self._ctx, pmin, pmax, q_cap, buf.ctypes.data, cap, ctypes.byref(n), ctypes.byref(st))
+        if rc and rc not in (-5, -6):
+            raise WilsonError(rc, "wl_rows")
+        return buf[: n.value].copy(), Stats.from_c(st)
+
+    def batch(self, ranges: Sequence[Tuple[int, int]], q_cap: int = 0, cap: int = 1 << 20):
+        n = len(ranges)
+        rr = (_Range * n)(*[_Range(a, b) for a, b in ranges])
+        out = (_RangeResult * n)()
+        res = (_Result * cap)()
+        nres = ctypes.c_size_t(0)
+        st = _Stats()
+        rc = self._L.wl_batch(self._ctx, rr, n, q_cap, out, res, cap, ctypes.byref(nres), ctypes.byref(st))
+        if rc:
+            raise WilsonError(rc, "wl_batch")
+        per_range = [dict(tested=o.tested, checksum=o.checksum, targets=tuple(o.targets), results=o.results,
+                          status=o.status) for o in out]
+        results = [(res[i].p, res[i].value) for i in range(min(nres.value, cap))]
+        return per_range, results, Stats.from_c(st)

@@ -1,0 +1,728 @@
+// wl_engine.cu -- host engine and C ABI of the Wilson-prime search.
+//
+// One search (or a batch of ranges) runs as:
+//   1. test primes: deterministic Miller-Rabin over each window [pmin, pmax)
+//      into an ordered list on the device (k_window_primes, k_compact);
+//   2. classification into (range, class) buckets with the reference's shared
+//      class target = the target of the first prime of the class
+//      (cl_wilson.cpp:1549-1586);
+//   3. the column cache: every prime below the largest needed column, sieved
+//      once per context on the device and kept resident (k_sieve_segments);
+//   4. the column sweep over splits of each bucket's columns (k_sweep), the
+//      consecutive-integer tail (k_iterate), and the combine + class lift +
+//      quotient (k_finish);
+//   5. results.txt lines (ascending p) and the checksum on the host
+//      (cl_wilson.cpp:872-900).
+#include <algorithm>
+#include <cerrno>
+#include <cstdlib>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "wilson.h"
+#include "wl_internal.h"
+
+using namespace wl;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+int ensure(DevBuf& b, size_t bytes) {
+    if (bytes <= b.cap && b.p) return 0;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t nb = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&b.p, nb) != cudaSuccess) {
+        cudaGetLastError();
+        return WL_ERR_NOMEM;
+    }
+    b.cap = nb;
+    return 0;
+}
+
+template <class T> T* as(DevBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+uint64_t pi_upper_bound(uint64_t x) {   // Rosser-Schoenfeld: pi(x) < 1.25506 x / ln x for x > 1
+    if (x < 64) return 64;
+    return (uint64_t)(1.2551 * (double)x / std::log((double)x)) + 64;
+}
+
+int limb_width(uint64_t pmax_incl) {
+    if (pmax_incl < (1ull << 31)) return 2;
+    if (pmax_incl < (1ull << 47)) return 3;
+    return 4;
+}
+
+}  // namespace
+
+#define CK(x)                                                        \
+    do {                                                             \
+        cudaError_t e_ = (x);                                        \
+        if (e_ != cudaSuccess) {                                     \
+            fprintf(stderr, "wilson: CUDA error %s at %s:%d\n",      \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return WL_ERR_CUDA;                                      \
+        }                                                            \
+    } while (0)
+
+#define RC(x)                      \
+    do {                           \
+        int r_ = (x);              \
+        if (r_) return r_;         \
+    } while (0)
+
+struct wl_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8] = {};
+    DevBuf base;            // odd primes < 65536 (sieving primes of the column sieve)
+    uint32_t nbase = 0;
+    DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
+    uint64_t ncols = 0, col_limit = 0;
+    DevBuf bitmap, segcount, offsets;
+    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, iitems, part, ipart, defs, rowout;
+    uint32_t launches = 0;
+    uint64_t h2d = 0, d2h = 0;
+    double ms_sieve = 0;
+};
+
+// ---------------------------------------------------------------------------
+// column cache
+// ---------------------------------------------------------------------------
+
+static int ensure_columns(wl_ctx* c, uint64_t limit) {
+    if (limit <= c->col_limit) return 0;
+    const uint64_t top = 1ull << 32;
+    if (limit > top) return WL_ERR_UNSUPPORTED;
+    uint64_t nl = std::max<uint64_t>(limit, std::min<uint64_t>(top, 2 * c->col_limit));
+    nl = (nl + SEG_SPAN - 1) / SEG_SPAN * SEG_SPAN;
+    if (nl > top) nl = top;
+    const uint32_t nseg = (uint32_t)(nl / SEG_SPAN);
+    RC(ensure(c->bitmap, (size_t)nseg * SEG_WORDS * 4));
+    RC(ensure(c->segcount, (size_t)nseg * 4));
+    RC(ensure(c->offsets, (size_t)(nseg + 1) * 8));
+    RC(ensure(c->cols, (size_t)pi_upper_bound(nl) * 4 + 64));
+    cudaEventRecord(c->ev[6], c->st);
+    launch_sieve_segments(0, nseg, nl, as<uint32_t>(c->base), c->nbase, as<uint32_t>(c->bitmap),
+                          as<uint32_t>(c->segcount), c->st);
+    launch_scan_counts(as<uint32_t>(c->segcount), nseg, 1, as<uint64_t>(c->offsets), c->st);
+    launch_compact(nseg, 0, as<uint32_t>(c->bitmap), as<uint64_t>(c->offsets), as<uint32_t>(c->cols), nullptr,
+                   c->st);
+    c->launches += 3;
+    static const uint32_t two = 2;
+    CK(cudaMemcpyAsync(as<uint32_t>(c->cols), &two, 4, cudaMemcpyHostToDevice, c->st));
+    uint64_t total = 0;
+    CK(cudaMemcpyAsync(&total, as<uint64_t>(c->offsets) + nseg, 8, cudaMemcpyDeviceToHost, c->st));
+    cudaEventRecord(c->ev[7], c->st);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+    c->ms_sieve += ms;
+    c->ncols = total;
+    c->col_limit = nl;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// the search pipeline over a set of ranges
+// ---------------------------------------------------------------------------
+
+struct RangeState {
+    uint64_t pmin, pmax, lo0;
+    uint32_t nseg;
+    uint64_t word_off, seg_off;
+    uint64_t tp_off = 0, ntp = 0;
+    uint64_t T[3] = { 0, 0, 0 };
+    uint64_t per_class[3] = { 0, 0, 0 };
+};
+
+struct HostBucket {
+    uint32_t range, type, L;
+    uint64_t T;
+    std::vector<uint64_t> primes;   // ascending
+    std::vector<uint32_t> src;      // index into the range's prime list
+};
+
+struct RunOut {
+    std::vector<wl_row> rows;             // all rows, ranges in order, ascending p within a range
+    std::vector<uint64_t> range_row_off;  // rows of range r: [off[r], off[r+1])
+    std::vector<uint64_t> range_targets;  // 3 per range
+    uint64_t pi_maxtarget = 0, cells = 0, tail = 0;
+};
+
+static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qcap, RunOut& out, wl_stats* st) {
+    const bool full = (qcap == 0);
+    c->launches = 0;
+    c->h2d = c->d2h = 0;
+    c->ms_sieve = 0;
+    for (size_t i = 0; i < nr; ++i) RC(wl_check_range(ranges[i].pmin, ranges[i].pmax));
+
+    cudaEventRecord(c->ev[0], c->st);
+
+    // ---- 1. test primes ----------------------------------------------------
+    std::vector<RangeState> rs(nr);
+    uint64_t words = 0, segs = 0;
+    for (size_t i = 0; i < nr; ++i) {
+        RangeState& r = rs[i];
+        r.pmin = ranges[i].pmin;
+        r.pmax = ranges[i].pmax;
+        r.lo0 = r.pmin & ~1ull;
+        r.nseg = (uint32_t)((r.pmax - r.lo0 + SEG_SPAN - 1) / SEG_SPAN);
+        r.word_off = words;
+        r.seg_off = segs;
+        words += (uint64_t)r.nseg * SEG_WORDS;
+        segs += r.nseg;
+    }
+    RC(ensure(c->bitmap, std::max<uint64_t>(words * 4, c->bitmap.cap)));
+    RC(ensure(c->segcount, std::max<uint64_t>(segs * 4, c->segcount.cap)));
+    RC(ensure(c->offsets, std::max<uint64_t>((segs + 1) * 8, c->offsets.cap)));
+    CK(cudaMemsetAsync(c->segcount.p, 0, segs * 4, c->st));
+    for (size_t i = 0; i < nr; ++i) {
+        RangeState& r = rs[i];
+        launch_window_primes(r.lo0, r.pmin, r.pmax, r.nseg, as<uint32_t>(c->bitmap) + r.word_off,
+                             as<uint32_t>(c->segcount) + r.seg_off, c->st);
+        c->launches++;
+    }
+    std::vector<uint32_t> segcnt(segs);
+    CK(cudaMemcpyAsync(segcnt.data(), c->segcount.p, segs * 4, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    c->d2h += segs * 4;
+    std::vector<uint64_t> offs(segs + 1);
+    uint64_t total = 0;
+    for (size_t i = 0; i < nr; ++i) {
+        RangeState& r = rs[i];
+        r.tp_off = total;
+        for (uint32_t s = 0; s < r.nseg; ++s) {
+            offs[r.seg_off + s] = total;
+            total += segcnt[r.seg_off + s];
+        }
+        r.ntp = total - r.tp_off;
+        if (r.ntp == 0) return WL_ERR_NOPRIMES;
+    }
+    offs[segs] = total;
+    if (total >= (1ull << 31)) return WL_ERR_UNSUPPORTED;
+    const uint32_t nrows = (uint32_t)total;
+    RC(ensure(c->tp, total * 8));
+    CK(cudaMemcpyAsync(c->offsets.p, offs.data(), (segs + 1) * 8, cudaMemcpyHostToDevice, c->st));
+    c->h2d += (segs + 1) * 8;
+    for (size_t i = 0; i < nr; ++i) {
+        RangeState& r = rs[i];
+        launch_compact(r.nseg, r.lo0, as<uint32_t>(c->bitmap) + r.word_off, as<uint64_t>(c->offsets) + r.seg_off,
+                       nullptr, as<uint64_t>(c->tp), c->st);
+        c->launches++;
+    }
+    std::vector<uint64_t> tps(total);
+    CK(cudaMemcpyAsync(tps.data(), c->tp.p, total * 8, cudaMemcpyDeviceToHost, c->st));
+    cudaEventRecord(c->ev[1], c->st);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    c->d2h += total * 8;
+
+    // ---- 2. classification and buckets ---------------------------------------
+    std::vector<HostBucket> hb;
+    hb.reserve(nr * 3);
+    for (size_t i = 0; i < nr; ++i) {
+        RangeState& r = rs[i];
+        int bidx[3] = { -1, -1, -1 };
+        const int L = limb_width(r.pmax - 1);
+        for (uint64_t k = 0; k < r.ntp; ++k) {
+            const uint64_t p = tps[r.tp_off + k];
+            uint32_t t;
+            uint64_t Tp;
+            if (p % 3 == 1) { t = 0; Tp = (p - 1) / 6; }
+            else if (p % 12 == 5) { t = 1; Tp = (p - 1) / 4; }
+            else if (p % 12 == 11) { t = 2; Tp = (p - 1) / 2; }
+            else return WL_ERR_ARG;   // p = 2, 3 never occur since pmin >= 5
+            if (bidx[t] < 0) {
+                bidx[t] = (int)hb.size();
+                HostBucket b;
+                b.range = (uint32_t)i;
+                b.type = t;
+                b.L = (uint32_t)L;
+                b.T = Tp;
+                hb.push_back(b);
+                r.T[t] = Tp;
+            }
+            hb[bidx[t]].primes.push_back(p);
+            hb[bidx[t]].src.push_back((uint32_t)k);
+            r.per_class[t]++;
+        }
+    }
+    // device order of buckets: by limb width, then range, then class
+    std::vector<uint32_t> border(hb.size());
+    for (size_t i = 0; i < hb.size(); ++i) border[i] = (uint32_t)i;
+    std::stable_sort(border.begin(), border.end(), [&](uint32_t a, uint32_t b) { return hb[a].L < hb[b].L; });
+
+    // ---- 3. columns ------------------------------------------------------------
+    uint64_t need = 0;
+    std::vector<uint64_t> keys(hb.size());
+    for (size_t i = 0; i < hb.size(); ++i) {
+        uint64_t key = hb[i].T;
+        if (!full && qcap - 1 < key) key = qcap - 1;
+        keys[i] = key;
+        need = std::max(need, key + 1);
+    }
+    // the largest class target of the first range (for pi(maxtarget))
+    uint64_t maxt0 = std::max(rs[0].T[0], std::max(rs[0].T[1], rs[0].T[2]));
+    if (full && need > (1ull << 32)) return WL_ERR_UNSUPPORTED;
+    RC(ensure_columns(c, need));
+    RC(ensure(c->keys, (hb.size() + 1) * 8));
+    RC(ensure(c->counts, (hb.size() + 1) * 8));
+    keys.push_back(full ? maxt0 : std::min(maxt0, qcap - 1));
+    CK(cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st));
+    launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->keys), (uint32_t)keys.size(),
+                     as<uint64_t>(c->counts), c->st);
+    c->launches++;
+    std::vector<uint64_t> ncol(keys.size());
+    CK(cudaMemcpyAsync(ncol.data(), c->counts.p, keys.size() * 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    c->h2d += keys.size() * 8;
+    c->d2h += keys.size() * 8;
+    out.pi_maxtarget = ncol.back();
+
+    // ---- 4. device layout: rows, buckets, splits, items ------------------------
+    std::vector<Bucket> db(hb.size());
+    std::vector<RowInfo> ri(nrows);
+    std::vector<uint64_t> row_src(nrows);    // global output index (range-major, ascending p)
+    double W = 0;
+    for (size_t i = 0; i < hb.size(); ++i) W += (double)hb[i].primes.size() * (double)ncol[i];
+    const double target_threads = (double)c->sms * 2048.0 * 4.0;
+    uint32_t row = 0;
+    uint64_t part_total = 0;
+    uint32_t def_total = 0;
+    out.cells = 0;
+    struct ItemGroup { int L, rpt; std::vector<SweepItem> items; };
+    std::vector<ItemGroup> groups;
+    auto group_for = [&](int L, int rpt) -> std::vector<SweepItem>& {
+        for (auto& g : groups) if (g.L == L && g.rpt == rpt) return g.items;
+        groups.push_back({ L, rpt, {} });
+        return groups.back().items;
+    };
+    for (uint32_t oi = 0; oi < border.size(); ++oi) {
+        const uint32_t i = border[oi];
+        const HostBucket& h = hb[i];
+        Bucket& b = db[oi];
+        b.T = h.T;
+        b.ncols = (uint32_t)ncol[i];
+        b.row_begin = row;
+        b.nrows = (uint32_t)h.primes.size();
+        b.L = h.L;
+        b.type = h.type;
+        b.range = h.range;
+        int rpt, tps;
+        if (b.nrows >= 512) { rpt = 2; tps = 256; }
+        else if (b.nrows >= 256) { rpt = 1; tps = 256; }
+        else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
+        uint64_t S = 1;
+        if (b.ncols > 0 && W > 0) {
+            S = (uint64_t)std::ceil((double)rpt * (double)b.ncols * target_threads / W);
+            const uint64_t min_split = 2048;
+            S = std::min<uint64_t>(S, std::max<uint64_t>(1, b.ncols / min_split));
+            S = std::max<uint64_t>(S, 1);
+        }
+        b.nsplit = (uint32_t)S;
+        b.part_base = part_total;
+        b.def_base = def_total;
+        part_total += S * b.nrows;
+        def_total += (uint32_t)S;
+        out.cells += (uint64_t)b.nrows * b.ncols;
+        auto& items = group_for((int)b.L, rpt);
+        if (tps == 256) {
+            const uint32_t tile = 256 * rpt;
+            for (uint32_t r0 = 0; r0 < b.nrows; r0 += tile)
+                for (uint32_t s = 0; s < S; ++s) items.push_back({ oi, r0, s, 256u });
+        } else {
+            const uint32_t per = 256 / tps;
+            for (uint32_t s = 0; s < S; s += per) items.push_back({ oi, 0, s, (uint32_t)tps });
+        }
+        for (uint32_t k = 0; k < b.nrows; ++k) {
+            RowInfo& x = ri[row + k];
+            x.p = h.primes[k];
+            x.type = h.type;
+            x.Tp = h.type == 0 ? (x.p - 1) / 6 : (h.type == 1 ? (x.p - 1) / 4 : (x.p - 1) / 2);
+            x.bucket = oi;
+            x.it_begin = 0;
+            x.it_count = 0;
+            row_src[row + k] = rs[h.range].tp_off + h.src[k];
+        }
+        row += b.nrows;
+    }
+    // consecutive-integer tail items (full search only)
+    std::vector<IterItem> it;
+    std::vector<std::pair<uint32_t, uint32_t>> it_groups;   // per limb width: [begin, end)
+    out.tail = 0;
+    if (full) {
+        uint64_t Wt = 0;
+        for (uint32_t r = 0; r < nrows; ++r) Wt += ri[r].Tp - db[ri[r].bucket].T;
+        out.tail = Wt;
+        const double tgt_items = (double)c->sms * 2048.0 * 2.0;
+        uint64_t K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / tgt_items));
+        K = std::min<uint64_t>(K, 1u << 30);
+        for (uint32_t r = 0; r < nrows; ++r) {
+            const uint64_t T = db[ri[r].bucket].T;
+            const uint64_t len = ri[r].Tp - T;
+            ri[r].it_begin = (uint32_t)it.size();
+            for (uint64_t a = 0; a < len; a += K) {
+                IterItem x;
+                x.start = T + 1 + a;
+                x.row = r;
+                x.len = (uint32_t)std::min<uint64_t>(K, len - a);
+                it.push_back(x);
+            }
+            ri[r].it_count = (uint32_t)(it.size() - ri[r].it_begin);
+        }
+    }
+
+    // ---- 5. upload and launch ----------------------------------------------------
+    size_t nitems_total = 0;
+    for (auto& g : groups) nitems_total += g.items.size();
+    RC(ensure(c->buckets, db.size() * sizeof(Bucket)));
+    RC(ensure(c->rowinfo, (size_t)nrows * sizeof(RowInfo)));
+    RC(ensure(c->rowmod, (size_t)nrows * sizeof(RowMod)));
+    RC(ensure(c->items, nitems_total * sizeof(SweepItem) + 16));
+    RC(ensure(c->iitems, it.size() * sizeof(IterItem) + 16));
+    RC(ensure(c->part, part_total * 16 + 16));
+    RC(ensure(c->ipart, it.size() * 16 + 16));
+    RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
+    RC(ensure(c->rowout, (size_t)nrows * sizeof(RowOut)));
+    CK(cudaMemcpyAsync(c->buckets.p, db.data(), db.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->rowinfo.p, ri.data(), (size_t)nrows * sizeof(RowInfo), cudaMemcpyHostToDevice, c->st));
+    std::vector<SweepItem> all_items;
+    all_items.reserve(nitems_total);
+    for (auto& g : groups) all_items.insert(all_items.end(), g.items.begin(), g.items.end());
+    if (!all_items.empty())
+        CK(cudaMemcpyAsync(c->items.p, all_items.data(), all_items.size() * sizeof(SweepItem),
+                           cudaMemcpyHostToDevice, c->st));
+    if (!it.empty())
+        CK(cudaMemcpyAsync(c->iitems.p, it.data(), it.size() * sizeof(IterItem), cudaMemcpyHostToDevice, c->st));
+    c->h2d += db.size() * sizeof(Bucket) + (size_t)nrows * sizeof(RowInfo) + all_items.size() * sizeof(SweepItem) +
+              it.size() * sizeof(IterItem);
+
+    launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
+    c->launches++;
+    cudaEventRecord(c->ev[2], c->st);
+    size_t ioff = 0;
+    for (auto& g : groups) {
+        launch_sweep(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
+                     as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint4>(c->part), as<Deficit>(c->defs), c->st);
+        if (!g.items.empty()) c->launches++;
+        ioff += g.items.size();
+    }
+    cudaEventRecord(c->ev[3], c->st);
+    // rows are ordered by limb width: one tail and one finish launch per width
+    uint32_t rb = 0;
+    std::vector<std::pair<int, std::pair<uint32_t, uint32_t>>> lgroups;   // L, [row begin, row end)
+    while (rb < nrows) {
+        const int L = (int)db[ri[rb].bucket].L;
+        uint32_t re = rb;
+        while (re < nrows && (int)db[ri[re].bucket].L == L) ++re;
+        lgroups.push_back({ L, { rb, re } });
+        rb = re;
+    }
+    for (auto& g : lgroups) {
+        const uint32_t ib = ri[g.second.first].it_begin;
+        const uint32_t last = g.second.second - 1;
+        const uint32_t ie = ri[last].it_begin + ri[last].it_count;
+        if (ie > ib) {
+            launch_iterate(g.first, as<IterItem>(c->iitems) + ib, ie - ib, as<RowMod>(c->rowmod),
+                           as<uint4>(c->ipart) + ib, c->st);
+            c->launches++;
+        }
+    }
+    cudaEventRecord(c->ev[4], c->st);
+    for (auto& g : lgroups) {
+        launch_finish(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                      as<uint4>(c->part), as<Deficit>(c->defs), as<IterItem>(c->iitems), as<uint4>(c->ipart),
+                      g.second.first, g.second.second - g.second.first, full ? 1 : 0, as<RowOut>(c->rowout), c->st);
+        c->launches++;
+    }
+    std::vector<RowOut> ro(nrows);
+    CK(cudaMemcpyAsync(ro.data(), c->rowout.p, (size_t)nrows * sizeof(RowOut), cudaMemcpyDeviceToHost, c->st));
+    c->d2h += (size_t)nrows * sizeof(RowOut);
+    cudaEventRecord(c->ev[5], c->st);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+
+    // ---- 6. gather rows in range order, ascending p ------------------------------
+    out.rows.assign(nrows, wl_row{});
+    for (uint32_t r = 0; r < nrows; ++r) {
+        wl_row& w = out.rows[row_src[r]];
+        w.p = ri[r].p;
+        w.s0 = ro[r].s0;
+        w.s1 = ro[r].s1;
+        w.rem = ro[r].rem;
+        w.quot = ro[r].quot;
+        w.type = ri[r].type;
+        w.status = ro[r].status;
+    }
+    out.range_row_off.assign(nr + 1, 0);
+    out.range_targets.assign(nr * 3, 0);
+    for (size_t i = 0; i < nr; ++i) {
+        out.range_row_off[i] = rs[i].tp_off;
+        for (int t = 0; t < 3; ++t) out.range_targets[i * 3 + t] = rs[i].T[t];
+    }
+    out.range_row_off[nr] = total;
+
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->tested = total;
+        for (size_t i = 0; i < nr; ++i)
+            for (int t = 0; t < 3; ++t) st->per_class[t] += rs[i].per_class[t];
+        for (int t = 0; t < 3; ++t) st->targets[t] = rs[0].T[t];
+        st->pi_maxtarget = out.pi_maxtarget;
+        st->cells = out.cells;
+        st->tail_steps = out.tail;
+        float a = 0;
+        cudaEventElapsedTime(&a, c->ev[0], c->ev[5]); st->ms_device = a;
+        cudaEventElapsedTime(&a, c->ev[0], c->ev[1]); st->ms_primes = a;
+        st->ms_sieve = c->ms_sieve;
+        cudaEventElapsedTime(&a, c->ev[2], c->ev[3]); st->ms_sweep = a;
+        cudaEventElapsedTime(&a, c->ev[3], c->ev[4]); st->ms_iterate = a;
+        cudaEventElapsedTime(&a, c->ev[4], c->ev[5]); st->ms_finish = a;
+        st->kernel_launches = c->launches;
+        st->h2d_bytes = c->h2d;
+        st->d2h_bytes = c->d2h;
+    }
+    return 0;
+}
+
+// results.txt value of one row (cl_wilson.cpp:872-898): 1 if it is a result line
+static int result_of(const wl_row& r, int32_t* value) {
+    const uint64_t negq = r.p - r.quot;
+    const uint64_t smallest = r.quot <= negq ? r.quot : negq;
+    if (r.quot == 0) { *value = 0; return 1; }
+    if (smallest < 1000) { *value = (smallest == r.quot) ? (int32_t)r.quot : -(int32_t)negq; return 1; }
+    return 0;
+}
+
+static int summarize(const RunOut& ro, size_t nr, bool full, wl_range_result* rr, wl_result* res, size_t cap,
+                     size_t* nres, wl_stats* st) {
+    size_t k = 0;
+    int err = 0;
+    uint64_t total_ck = 0;
+    uint32_t total_res = 0;
+    for (size_t i = 0; i < nr; ++i) {
+        uint64_t ck = 0;
+        uint32_t cnt = 0, status = 0;
+        for (uint64_t j = ro.range_row_off[i]; j < ro.range_row_off[i + 1]; ++j) {
+            const wl_row& r = ro.rows[j];
+            if (full) {
+                ck += r.p + r.rem + r.quot;
+                int32_t v;
+                if (result_of(r, &v)) {
+                    if (res && k < cap) { res[k].p = r.p; res[k].value = v; res[k].pad = 0; }
+                    ++k;
+                    ++cnt;
+                }
+                if (r.status && !status) status = r.status;
+            } else {
+                ck += r.p + r.s0 + r.s1;
+            }
+        }
+        if (rr) {
+            rr[i].tested = ro.range_row_off[i + 1] - ro.range_row_off[i];
+            rr[i].checksum = ck;
+            for (int t = 0; t < 3; ++t) rr[i].targets[t] = ro.range_targets[i * 3 + t];
+            rr[i].results = cnt;
+            rr[i].status = status;
+        }
+        total_ck += ck;
+        total_res += cnt;
+        if (status == 1 && !err) err = WL_ERR_WILSON_CHECK;
+        if (status == 2 && !err) err = WL_ERR_NO_REPR;
+    }
+    if (nres) *nres = k;
+    if (st) {
+        st->checksum = total_ck;
+        st->results = total_res;
+    }
+    if (err) return err;
+    if (res && k > cap) return WL_ERR_CAPACITY;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char* wl_strerror(int code) {
+    switch (code) {
+        case WL_OK: return "ok";
+        case WL_ERR_ARG: return "invalid argument or range";
+        case WL_ERR_CUDA: return "CUDA error";
+        case WL_ERR_NOPRIMES: return "there are no primes to test in this range!";
+        case WL_ERR_UNSUPPORTED: return "configuration not supported by this build";
+        case WL_ERR_WILSON_CHECK: return "Wilson quotient check failed";
+        case WL_ERR_NO_REPR: return "representation a, c or u not found";
+        case WL_ERR_CAPACITY: return "result buffer too small";
+        case WL_ERR_NOMEM: return "device allocation failed";
+        default: return "unknown error";
+    }
+}
+
+int wl_check_range(uint64_t pmin, uint64_t pmax) {
+    if (pmin < 5 || pmax > WL_MAXP || pmin >= pmax) return WL_ERR_ARG;
+    if (pmax - pmin > WL_MAX_WIDTH) return WL_ERR_ARG;
+    return 0;
+}
+
+int wl_open(int device, wl_ctx** out) {
+    if (!out) return WL_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return WL_ERR_CUDA;
+    }
+    wl_ctx* c = new wl_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    // odd primes below 2^16: the sieving primes of the column sieve (q < 2^32)
+    std::vector<uint8_t> comp(65536, 0);
+    std::vector<uint32_t> base;
+    for (uint32_t i = 3; i < 65536; i += 2) {
+        if (comp[i]) continue;
+        base.push_back(i);
+        for (uint32_t j = i * i; j < 65536; j += 2 * i) comp[j] = 1;
+    }
+    c->nbase = (uint32_t)base.size();
+    if (ensure(c->base, base.size() * 4) ||
+        cudaMemcpy(c->base.p, base.data(), base.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        wl_close(c);
+        return WL_ERR_CUDA;
+    }
+    *out = c;
+    return 0;
+}
+
+void wl_close(wl_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    DevBuf* bufs[] = { &c->base, &c->cols, &c->bitmap, &c->segcount, &c->offsets, &c->tp, &c->keys, &c->counts,
+                       &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->iitems, &c->part, &c->ipart,
+                       &c->defs, &c->rowout };
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+void* wl_stream(wl_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int wl_search(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_cap, wl_result* results, size_t cap,
+              wl_stats* stats) {
+    if (!c) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    wl_range r = { pmin, pmax };
+    RunOut ro;
+    RC(run_ranges(c, &r, 1, q_cap, ro, stats));
+    return summarize(ro, 1, q_cap == 0, nullptr, results, cap, nullptr, stats);
+}
+
+int wl_rows(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_cap, wl_row* rows, size_t cap, size_t* nrows,
+            wl_stats* stats) {
+    if (!c) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    wl_range r = { pmin, pmax };
+    RunOut ro;
+    RC(run_ranges(c, &r, 1, q_cap, ro, stats));
+    if (nrows) *nrows = ro.rows.size();
+    if (rows) {
+        const size_t n = std::min(cap, ro.rows.size());
+        memcpy(rows, ro.rows.data(), n * sizeof(wl_row));
+    }
+    int e = summarize(ro, 1, q_cap == 0, nullptr, nullptr, 0, nullptr, stats);
+    if (e) return e;
+    if (rows && cap < ro.rows.size()) return WL_ERR_CAPACITY;
+    return 0;
+}
+
+int wl_batch(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, wl_range_result* out,
+             wl_result* results, size_t cap, size_t* nresults, wl_stats* stats) {
+    if (!c || !ranges || n == 0) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    RunOut ro;
+    RC(run_ranges(c, ranges, n, q_cap, ro, stats));
+    return summarize(ro, n, q_cap == 0, out, results, cap, nresults, stats);
+}
+
+// parse_uint64 (putil.c:34-116): decimal/hex/octal with K,M,G,T,P (x1000),
+// e<n> (x10^n), k,m,g,t,p (x2^10) and b<n> (x2^n) suffixes.
+int wl_parse_uint64(uint64_t* result, const char* str, uint64_t lo, uint64_t hi) {
+    if (!result || !str) return -1;
+    errno = 0;
+    char* tail = nullptr;
+    uint64_t num = strtoull(str, &tail, 0);
+    if (errno != 0 || num > hi) return -2;
+    uint32_t expt = 0;
+    switch (*tail) {
+        case 'P': expt += 3; [[fallthrough]];
+        case 'T': expt += 3; [[fallthrough]];
+        case 'G': expt += 3; [[fallthrough]];
+        case 'M': expt += 3; [[fallthrough]];
+        case 'K':
+            expt += 3;
+            if (tail[1] != '\0') return -1;
+            for (; expt > 0; expt -= 3) {
+                if (num > hi / 1000) return -2;
+                num *= 1000;
+            }
+            break;
+        case 'e':
+        case 'E':
+            expt = (uint32_t)strtoul(tail + 1, &tail, 0);
+            if (errno != 0) return -2;
+            if (*tail != '\0') return -1;
+            while (expt-- > 0) {
+                if (num > hi / 10) return -2;
+                num *= 10;
+            }
+            break;
+        case 'p': expt += 10; [[fallthrough]];
+        case 't': expt += 10; [[fallthrough]];
+        case 'g': expt += 10; [[fallthrough]];
+        case 'm': expt += 10; [[fallthrough]];
+        case 'k':
+            expt += 10;
+            if (tail[1] != '\0') return -1;
+            if (num > (hi >> expt)) return -2;
+            num <<= expt;
+            break;
+        case 'b':
+        case 'B':
+            expt = (uint32_t)strtoul(tail + 1, &tail, 0);
+            if (errno != 0) return -2;
+            if (*tail != '\0') return -1;
+            while (expt-- > 0) {
+                if (num > (hi >> 1)) return -2;
+                num <<= 1;
+            }
+            break;
+        case '\0':
+            break;
+        default:
+            return -1;
+    }
+    if (num < lo) return -2;
+    *result = num;
+    return 0;
+}
+
+}  // extern "C"

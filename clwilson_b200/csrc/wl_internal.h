@@ -1,0 +1,91 @@
+// wl_internal.h -- data layout shared by the CUDA kernels and the host engine.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace wl {
+
+// Sieve geometry: one CTA sieves SEG_SPAN consecutive integers, odd ones only,
+// as a SEG_WORDS x 32-bit bitmap in shared memory.
+constexpr uint32_t SEG_SPAN = 1u << 18;
+constexpr uint32_t SEG_BITS = SEG_SPAN / 2;
+constexpr uint32_t SEG_WORDS = SEG_BITS / 32;
+
+// Per-row modulus constants.  Only the first L limbs of n are meaningful.
+struct __align__(32) RowMod {
+    uint32_t n[4];     // n = p^2, little-endian 32-bit limbs
+    uint32_t ninv;     // -n^-1 mod 2^32
+    uint32_t pad;
+    uint64_t p;
+};
+
+// A bucket: the test primes of one (range, residue class).  All rows of a
+// bucket share the class target T and so the column set (sieving primes
+// q <= T, q < q_cap) and the Legendre exponents v_q(T!).
+struct Bucket {
+    uint64_t T;          // shared class target (cl_wilson.cpp:1557-1579)
+    uint64_t part_base;  // partial products: part[part_base + s*nrows + r]
+    uint32_t ncols;      // columns used: cols[0 .. ncols)
+    uint32_t row_begin;  // first row (global index) of this bucket
+    uint32_t nrows;
+    uint32_t nsplit;     // column splits
+    uint32_t def_base;   // split deficits: defs[def_base + s]
+    uint32_t L;          // limb width (2, 3, 4)
+    uint32_t type;       // 0: p = 1 mod 3, 1: p = 5 mod 12, 2: p = 11 mod 12
+    uint32_t range;      // index of the range this bucket belongs to
+};
+
+// One CTA of the column sweep: threads [k*tps, (k+1)*tps) work on split
+// split0 + k; thread i of a group takes rows row0 + i + j*tps, j < RPT.
+struct SweepItem {
+    uint32_t bucket, row0, split0, tps;
+};
+
+// One thread of the consecutive-integer tail: N = start .. start+len-1.
+struct IterItem {
+    uint64_t start;
+    uint32_t row;
+    uint32_t len;
+};
+
+// Per-row state beyond the modulus.
+struct RowInfo {
+    uint64_t p;
+    uint64_t Tp;         // own target (p-1)/6, /4 or /2
+    uint32_t bucket;
+    uint32_t it_begin;   // iterate items [it_begin, it_begin + it_count)
+    uint32_t it_count;
+    uint32_t type;
+};
+
+// Per-row output.
+struct RowOut {
+    uint64_t s0, s1;     // digits of T_p! mod p^2 (or of the capped partial product)
+    uint64_t rem, quot;  // ((p-1)! + 1) mod p^2 = rem + p*quot
+    uint32_t status;     // 0 ok, 1 rem != 0, 2 no representation found
+    uint32_t pad;
+};
+
+struct Deficit { uint64_t lo, hi; };
+
+// Launch wrappers (wl_kernels.cu).  All are asynchronous on `st`.
+void launch_sieve_segments(uint32_t seg0, uint32_t nseg, uint64_t limit, const uint32_t* base,
+                           uint32_t nbase, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
+void launch_scan_counts(const uint32_t* counts, uint32_t n, uint64_t first, uint64_t* offsets,
+                        cudaStream_t st);
+void launch_compact(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets,
+                    uint32_t* out32, uint64_t* out64, cudaStream_t st);
+void launch_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t* bitmap,
+                          uint32_t* seg_count, cudaStream_t st);
+void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys,
+                      uint64_t* out, cudaStream_t st);
+void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
+void launch_sweep(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out,
+                    cudaStream_t st);
+void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods,
+                   const uint4* part, const Deficit* defs, const IterItem* iitems, const uint4* ipart,
+                   uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st);
+
+}  // namespace wl

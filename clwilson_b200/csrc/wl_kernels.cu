@@ -1,0 +1,714 @@
+// wl_kernels.cu -- sm_100a kernels of the Wilson-prime engine.
+//
+//   k_sieve_segments / k_compact   sieving primes q < 2^32 (the columns)
+//   k_window_primes                test primes in [pmin, pmax) (the rows)
+//   k_setup_rows                   per-row modulus constants (setup.cl)
+//   k_sweep<L,RPT>                 prod_{q <= T} q^{v_q(T!)} over a column split
+//                                  (mulsmall.cl / mullarge.cl / reduce.cl)
+//   k_iterate<L>                   prod of consecutive integers (iterate.cl)
+//   k_finish<L>                    combine splits + tail, class lift, quotient
+//                                  (cl_wilson.cpp:691-900, find.cl)
+#include "wl_internal.h"
+#include "wl_arith.cuh"
+
+namespace wl {
+
+// ===========================================================================
+// Column sieve: all primes below `limit` (limit <= 2^32), odd-only segmented
+// sieve of Eratosthenes with the bitmap in shared memory.
+// ===========================================================================
+
+constexpr uint32_t SIEVE_THREADS = 512;
+constexpr uint32_t SMALL_PRIME_COOP = 1024;   // primes below this are marked cooperatively
+
+__global__ void __launch_bounds__(SIEVE_THREADS)
+k_sieve_segments(uint32_t seg0, uint64_t limit, const uint32_t* __restrict__ base, uint32_t nbase,
+                 uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
+    __shared__ uint32_t marks[SEG_WORDS];
+    __shared__ uint32_t warp_sum[SIEVE_THREADS / 32];
+    const uint32_t seg = seg0 + blockIdx.x;
+    const uint64_t lo = (uint64_t)seg * SEG_SPAN;
+    const uint64_t hi = lo + SEG_SPAN;
+    for (uint32_t i = threadIdx.x; i < SEG_WORDS; i += blockDim.x) marks[i] = 0;
+    __syncthreads();
+
+    // base primes are odd primes in ascending order; stop once b^2 >= hi
+    uint32_t k = 0;
+    // cooperative marking for small primes: thread t marks multiples t, t+T, ...
+    for (; k < nbase; ++k) {
+        const uint64_t b = base[k];
+        if (b >= SMALL_PRIME_COOP || b * b >= hi) break;
+        uint64_t m = (lo + b - 1) / b * b;
+        if (m < b * b) m = b * b;
+        if (!(m & 1)) m += b;
+        if (m >= hi) continue;
+        const uint32_t i0 = (uint32_t)((m - lo) >> 1);
+        for (uint32_t i = i0 + threadIdx.x * (uint32_t)b; i < SEG_BITS; i += blockDim.x * (uint32_t)b)
+            atomicOr(&marks[i >> 5], 1u << (i & 31));
+    }
+    // one larger prime per thread
+    for (uint32_t kk = k + threadIdx.x; kk < nbase; kk += blockDim.x) {
+        const uint64_t b = base[kk];
+        if (b * b >= hi) break;
+        uint64_t m = (lo + b - 1) / b * b;
+        if (m < b * b) m = b * b;
+        if (!(m & 1)) m += b;
+        for (uint64_t i = (m - lo) >> 1; i < SEG_BITS; i += b)
+            atomicOr(&marks[i >> 5], 1u << (i & 31));
+    }
+    __syncthreads();
+
+    uint32_t cnt = 0;
+    for (uint32_t w = threadIdx.x; w < SEG_WORDS; w += blockDim.x) {
+        uint32_t prime_bits = ~marks[w];
+        const uint64_t first = lo + (uint64_t)w * 64 + 1;           // number of bit 0
+        if (first + 62 >= limit) {                                   // clip to < limit
+            uint32_t keep = 0;
+            for (int bI = 0; bI < 32; ++bI)
+                if (first + 2 * (uint64_t)bI < limit) keep |= 1u << bI;
+            prime_bits &= keep;
+        }
+        if (seg == 0 && w == 0) prime_bits &= ~1u;                  // 1 is not prime
+        bitmap[(uint64_t)blockIdx.x * SEG_WORDS + w] = prime_bits;
+        cnt += __popc(prime_bits);
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (uint32_t i = 0; i < blockDim.x / 32; ++i) s += warp_sum[i];
+        seg_count[blockIdx.x] = s;
+    }
+}
+
+// Exclusive scan of per-segment counts (single CTA), offsets[i] = first + sum_{j<i} counts[j];
+// offsets[n] = total.
+__global__ void __launch_bounds__(1024)
+k_scan_counts(const uint32_t* __restrict__ counts, uint32_t n, uint64_t first, uint64_t* __restrict__ offsets) {
+    __shared__ uint64_t part[1024];
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+    uint64_t s = 0;
+    for (uint32_t i = b; i < e; ++i) s += counts[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+        uint64_t v = (threadIdx.x >= off) ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint64_t run = first + (threadIdx.x ? part[threadIdx.x - 1] : 0);
+    for (uint32_t i = b; i < e; ++i) { offsets[i] = run; run += counts[i]; }
+    if (threadIdx.x == blockDim.x - 1) offsets[n] = first + part[blockDim.x - 1];
+}
+
+// Ordered write-out of the numbers whose bit is set: segment s covers odd
+// numbers lo0 + s*span + 2i + 1.  Writes 32-bit or 64-bit values.
+constexpr uint32_t COMPACT_THREADS = 256;
+__global__ void __launch_bounds__(COMPACT_THREADS)
+k_compact(uint64_t lo0, uint32_t span, const uint32_t* __restrict__ bitmap, const uint64_t* __restrict__ offsets,
+          uint32_t* __restrict__ out32, uint64_t* __restrict__ out64) {
+    __shared__ uint32_t wsum[COMPACT_THREADS / 32];
+    constexpr uint32_t WPT = SEG_WORDS / COMPACT_THREADS;   // words per thread
+    const uint32_t seg = blockIdx.x;
+    const uint32_t* bm = bitmap + (uint64_t)seg * SEG_WORDS + threadIdx.x * WPT;
+    uint32_t words[WPT];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < WPT; ++i) { words[i] = bm[i]; cnt += __popc(words[i]); }
+    // block exclusive scan of cnt
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (uint32_t i = 0; i < wid; ++i) wbase += wsum[i];
+    uint64_t pos = offsets[seg] + wbase + incl - cnt;
+    const uint64_t lo = lo0 + (uint64_t)seg * span;
+#pragma unroll
+    for (uint32_t i = 0; i < WPT; ++i) {
+        uint32_t w = words[i];
+        const uint64_t base_n = lo + (uint64_t)(threadIdx.x * WPT + i) * 64 + 1;
+        while (w) {
+            const int bI = __ffs(w) - 1;
+            w &= w - 1;
+            const uint64_t v = base_n + 2 * (uint64_t)bI;
+            if (out32) out32[pos] = (uint32_t)v;
+            else out64[pos] = v;
+            ++pos;
+        }
+    }
+}
+
+// ===========================================================================
+// Test primes: deterministic Miller-Rabin on every odd n in [lo, hi).
+// Bitmap layout as the sieve: segment s covers odd numbers lo0 + s*SEG_SPAN + 2i + 1.
+// ===========================================================================
+
+__device__ bool is_prime64(uint64_t n) {
+    if (n < 2) return false;
+    const uint32_t small[] = { 2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71 };
+#pragma unroll
+    for (int i = 0; i < 20; ++i) {
+        if (n == small[i]) return true;
+        if (n % small[i] == 0) return false;
+    }
+    Mod64 M;
+    M.init(n);
+    uint64_t d = n - 1;
+    int s = __ffsll((long long)d) - 1;
+    d >>= s;
+    const uint64_t minus1 = M.to(n - 1);
+    // bases of J. Sinclair: deterministic for n < 2^64
+    const uint64_t bases[7] = { 2, 325, 9375, 28178, 450775, 9780504, 1795265022 };
+    for (int i = 0; i < 7; ++i) {
+        const uint64_t a = bases[i] % n;
+        if (a == 0) continue;
+        uint64_t x = red64(M.pow(M.to(a), d), n);
+        if (x == M.one % n || x == minus1 % n) continue;
+        bool ok = false;
+        for (int r = 1; r < s; ++r) {
+            x = red64(M.mul(x, x), n);
+            if (x == minus1 % n) { ok = true; break; }
+        }
+        if (!ok) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(256)
+k_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
+    // one thread per odd number; a warp produces one bitmap word
+    const uint64_t bit = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nval = lo0 + 2 * bit + 1;
+    const bool pr = (nval >= lo && nval < hi) ? is_prime64(nval) : false;
+    const uint32_t word = __ballot_sync(0xffffffffu, pr);
+    if ((threadIdx.x & 31) == 0) {
+        bitmap[bit >> 5] = word;
+        if (word) atomicAdd(&seg_count[bit / SEG_BITS], (uint32_t)__popc(word));
+    }
+}
+
+// ===========================================================================
+// Count of columns <= key (binary search over the sorted column array).
+// ===========================================================================
+
+__global__ void k_count_leq(const uint32_t* __restrict__ cols, uint64_t ncols, const uint64_t* __restrict__ keys,
+                            uint32_t nkeys, uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nkeys) return;
+    const uint64_t key = keys[i];
+    uint64_t a = 0, b = ncols;          // first index with cols[idx] > key
+    while (a < b) {
+        uint64_t m = (a + b) >> 1;
+        if ((uint64_t)cols[m] <= key) a = m + 1; else b = m;
+    }
+    out[i] = a;
+}
+
+// ===========================================================================
+// Row setup: n = p^2 and -n^-1 mod 2^32 (setup.cl:18-45 computes the
+// reference's own per-prime constants; these are this engine's).
+// ===========================================================================
+
+__global__ void k_setup_rows(const RowInfo* __restrict__ info, uint32_t nrows, RowMod* __restrict__ mods) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const uint64_t p = info[i].p;
+    const u128 n = (u128)p * p;
+    RowMod r;
+    r.n[0] = (uint32_t)n;
+    r.n[1] = (uint32_t)(n >> 32);
+    r.n[2] = (uint32_t)(n >> 64);
+    r.n[3] = (uint32_t)(n >> 96);
+    uint32_t x = r.n[0];                // n^-1 mod 2^32 by Newton
+    for (int k = 0; k < 5; ++k) x *= 2u - r.n[0] * x;
+    r.ninv = 0u - x;
+    r.pad = 0;
+    r.p = p;
+    mods[i] = r;
+}
+
+// ===========================================================================
+// Column sweep.  For the bucket's target T and a split [c0, c1) of the
+// ascending column array (primes q <= T), each row computes
+//     C = prod_{c0 <= i < c1} q_i^{e_i},   e_i = v_{q_i}(T!)  (Legendre),
+// by the prefix-product identity: with P_i = q_c0 ... q_i and the exponents
+// non-increasing, C = prod_{i: e_i > e_{i+1}} P_i^{e_i - e_{i+1}} (e_{c1} = 0).
+// Each prime therefore costs one cell; a fold A *= P^d happens only where the
+// exponent drops, which for q > sqrt(T) is once per distinct floor(T/q).
+// Fold points depend on T only, so all rows of the bucket fold together.
+// Every cell drops a factor 2^32 and every full product 2^(32L); the total
+// ("deficit") is identical for all rows of a split and stored once per split.
+// ===========================================================================
+
+__device__ __forceinline__ uint64_t legendre(uint64_t T, uint64_t q) {
+    uint64_t e = 0, qq = q;
+    while (true) {
+        e += T / qq;
+        if (qq > T / q) break;
+        qq *= q;
+    }
+    return e;
+}
+
+template <int L>
+__device__ __forceinline__ void fold_pow(Res<L>& A, const Res<L>& P, uint64_t d, const uint32_t* n, uint32_t ninv) {
+    Res<L> Y = P;
+    const int top = 63 - __clzll((long long)d);
+    for (int b = top - 1; b >= 0; --b) {
+        Y = mont_mul<L>(Y, Y, n, ninv);
+        if ((d >> b) & 1) Y = mont_mul<L>(Y, P, n, ninv);
+    }
+    A = mont_mul<L>(A, Y, n, ninv);
+}
+
+template <int L, int RPT>
+__global__ void __launch_bounds__(256)
+k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
+        const uint32_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
+    const SweepItem it = items[blockIdx.x];
+    const Bucket bk = buckets[it.bucket];
+    const uint32_t s = it.split0 + threadIdx.x / it.tps;
+    if (s >= bk.nsplit) return;
+    const uint32_t rl = it.row0 + threadIdx.x % it.tps;
+
+    uint32_t n[RPT][L];
+    uint32_t ninv[RPT];
+    bool live[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        const uint32_t r = rl + j * it.tps;
+        live[j] = r < bk.nrows;
+        const RowMod m = mods[bk.row_begin + (live[j] ? r : 0)];
+#pragma unroll
+        for (int k = 0; k < L; ++k) n[j][k] = m.n[k];
+        ninv[j] = m.ninv;
+    }
+
+    const uint64_t T = bk.T;
+    const uint64_t c0 = (uint64_t)bk.ncols * s / bk.nsplit;
+    const uint64_t c1 = (uint64_t)bk.ncols * (s + 1) / bk.nsplit;
+
+    Res<L> P[RPT], A[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) { set_small<L>(P[j], 1); set_small<L>(A[j], 1); }
+    u128 def = 0;
+
+    if (c0 < c1) {
+        const uint64_t qf = cols[c0];
+        uint64_t e_cur = legendre(T, qf);
+        uint64_t thr = (qf * qf > T) ? T / e_cur : qf;
+        uint64_t cells = 0;
+        uint64_t c = c0;
+        while (c < c1) {
+            if (((c & 3) == 0) && c + 4 <= c1) {
+                const uint4 g = __ldg(reinterpret_cast<const uint4*>(cols + c));
+                if ((uint64_t)g.w <= thr) {
+                    if (L == 2 || g.w < 0x80000000u) {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            cell(P[j], g.x, n[j], ninv[j]);
+                            cell(P[j], g.y, n[j], ninv[j]);
+                            cell(P[j], g.z, n[j], ninv[j]);
+                            cell(P[j], g.w, n[j], ninv[j]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            cell_wide<L>(P[j], g.x, n[j], ninv[j]);
+                            cell_wide<L>(P[j], g.y, n[j], ninv[j]);
+                            cell_wide<L>(P[j], g.z, n[j], ninv[j]);
+                            cell_wide<L>(P[j], g.w, n[j], ninv[j]);
+                        }
+                    }
+                    c += 4;
+                    cells += 4;
+                    continue;
+                }
+            }
+            const uint32_t q = __ldg(cols + c);
+            if ((uint64_t)q > thr) {
+                const uint64_t e_new = legendre(T, q);
+                const uint64_t d = e_cur - e_new;
+                if (d) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
+                    def += (u128)d * (32 * cells + 32 * L);
+                }
+                e_cur = e_new;
+                thr = ((uint64_t)q * q > T) ? T / e_new : q;
+            }
+            if (L == 2 || q < 0x80000000u) {
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) cell(P[j], q, n[j], ninv[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) cell_wide<L>(P[j], q, n[j], ninv[j]);
+            }
+            ++c;
+            ++cells;
+        }
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], e_cur, n[j], ninv[j]);
+        def += (u128)e_cur * (32 * cells + 32 * L);
+    }
+
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        if (!live[j]) continue;
+        const uint32_t r = rl + j * it.tps;
+        uint4 o;
+        o.x = A[j].w[0];
+        o.y = A[j].w[1];
+        o.z = L > 2 ? A[j].w[2 < L ? 2 : 0] : 0;
+        o.w = L > 3 ? A[j].w[3 < L ? 3 : 0] : 0;
+        part[bk.part_base + (uint64_t)s * bk.nrows + r] = o;
+    }
+    if (it.row0 == 0 && threadIdx.x % it.tps == 0) {
+        Deficit dd;
+        dd.lo = (uint64_t)def;
+        dd.hi = (uint64_t)(def >> 64);
+        defs[bk.def_base + s] = dd;
+    }
+}
+
+// ===========================================================================
+// Consecutive-integer tail: prod_{N = start}^{start+len-1} N  (iterate.cl:30-43)
+// ===========================================================================
+
+template <int L>
+__global__ void __launch_bounds__(256)
+k_iterate(const IterItem* __restrict__ items, uint32_t nitems, const RowMod* __restrict__ mods, uint4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    const IterItem it = items[i];
+    const RowMod m = mods[it.row];
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    Res<L> acc;
+    set_small<L>(acc, 1);
+    const uint64_t last = it.start + it.len - 1;
+    if (last < 0x80000000ull) {
+        uint32_t N = (uint32_t)it.start;
+        uint32_t k = 0;
+        for (; k + 4 <= it.len; k += 4, N += 4) {
+            cell(acc, N, n, m.ninv);
+            cell(acc, N + 1, n, m.ninv);
+            cell(acc, N + 2, n, m.ninv);
+            cell(acc, N + 3, n, m.ninv);
+        }
+        for (; k < it.len; ++k, ++N) cell(acc, N, n, m.ninv);
+    } else {
+        uint64_t N = it.start;
+        for (uint32_t k = 0; k < it.len; ++k, ++N) cell64<L>(acc, N, n, m.ninv);
+    }
+    uint4 o;
+    o.x = acc.w[0];
+    o.y = acc.w[1];
+    o.z = L > 2 ? acc.w[2 < L ? 2 : 0] : 0;
+    o.w = L > 3 ? acc.w[3 < L ? 3 : 0] : 0;
+    out[i] = o;
+}
+
+// ===========================================================================
+// Finish: combine the split partials and the tail, restore the tracked
+// power of two, and (full search) lift T_p! to (p-1)! with the class formula
+// (cl_wilson.cpp:731-870), add 1, and split into rem + p*quot.
+// ===========================================================================
+
+// digits of v < p^2 in base p: v = d0 + p*d1
+template <int L>
+__device__ void digits_base_p(const Res<L>& v, uint64_t p, uint64_t* d0, uint64_t* d1) {
+    // remainder by bit-serial long division (runs once per row)
+    uint64_t r = 0;
+    for (int i = 32 * L - 1; i >= 0; --i) {
+        const uint32_t bitv = (v.w[i >> 5] >> (i & 31)) & 1u;
+        // r < p < 2^62, so 2r + 1 fits
+        r = (r << 1) | bitv;
+        if (r >= p) r -= p;
+    }
+    // exact quotient (v - r) / p modulo 2^64; the true quotient is < p < 2^64
+    uint64_t vlo = (uint64_t)v.w[0] | ((uint64_t)v.w[1] << 32);
+    const uint64_t pinv = inv64(p);
+    *d0 = r;
+    *d1 = (vlo - r) * pinv;
+}
+
+// Cornacchia: x^2 + d*y^2 = p given r0^2 = -d (mod p)
+__device__ bool cornacchia(uint64_t p, uint64_t d, uint64_t r0, uint64_t* x, uint64_t* y) {
+    if (r0 <= p / 2) r0 = p - r0;
+    uint64_t a = p, b = r0;
+    const uint64_t lim = isqrt64(p);
+    while (b > lim) { uint64_t t = a % b; a = b; b = t; }
+    const uint64_t rest = p - b * b;
+    if (rest % d) return false;
+    const uint64_t yy = rest / d, yr = isqrt64(yy);
+    if (yr * yr != yy) return false;
+    *x = b;
+    *y = yr;
+    return true;
+}
+
+// a with p = a^2 + b^2 (a odd, sign a = 1 mod 4: find.cl:52-58, only a^2 is used)
+__device__ bool find_a(uint64_t p, int64_t* out) {
+    Mod64 M;
+    M.init(p);
+    const uint64_t minus1 = p - 1;
+    for (uint64_t g = 2; g < 200; ++g) {
+        if (M.from(M.pow(M.to(g), (p - 1) / 2)) != minus1) continue;
+        const uint64_t r = M.from(M.pow(M.to(g), (p - 1) / 4));
+        uint64_t x, y;
+        if (!cornacchia(p, 1, r, &x, &y)) return false;
+        const uint64_t a = (x & 1) ? x : y;
+        *out = (a % 4 == 3) ? -(int64_t)a : (int64_t)a;
+        return true;
+    }
+    return false;
+}
+
+// c with 4p = c^2 + 27d^2 (c = 1 mod 3) and u with 4p = u^2 + 3v^2 (u = umod mod 3),
+// the sign rules of find.cl:77-83, 101-107 and cl_wilson.cpp:634
+__device__ bool find_cu(uint64_t p, int64_t* c_out, int64_t* u_out) {
+    Mod64 M;
+    M.init(p);
+    for (uint64_t g = 2; g < 200; ++g) {
+        const uint64_t w = M.from(M.pow(M.to(g), (p - 1) / 3));
+        if (w == 1) continue;
+        const uint64_t r = (2 * w + 1) % p;            // sqrt(-3) mod p
+        uint64_t x, y;
+        if (!cornacchia(p, 3, r, &x, &y)) return false;
+        const int64_t X = (int64_t)x, Y = (int64_t)y;
+        const int64_t us[3] = { 2 * X, X + 3 * Y, X - 3 * Y };
+        const int64_t vs[3] = { 2 * Y, X - Y, X + Y };
+        const uint32_t umod = (((p - 1) / 6) % 2 == 0) ? 1 : 2;
+        const uint64_t u = (uint64_t)(us[0] < 0 ? -us[0] : us[0]);
+        *u_out = (u % 3 == umod) ? (int64_t)u : -(int64_t)u;
+        for (int k = 0; k < 3; ++k) {
+            const int64_t v = vs[k] < 0 ? -vs[k] : vs[k];
+            if (v % 3 == 0) {
+                const uint64_t c = (uint64_t)(us[k] < 0 ? -us[k] : us[k]);
+                *c_out = (c % 3 == 2) ? -(int64_t)c : (int64_t)c;
+                return true;
+            }
+        }
+        return false;
+    }
+    return false;
+}
+
+template <int L>
+__device__ __forceinline__ Res<L> mont_of_signed(int64_t v, const Res<L>& R2, const uint32_t* n, uint32_t ninv) {
+    Res<L> x;
+    set_small<L>(x, (uint64_t)(v < 0 ? -v : v));
+    x = mont_mul<L>(x, R2, n, ninv);
+    if (v < 0) {
+        Res<L> z;
+        set_small<L>(z, 0);
+        x = sub_mod2n<L>(z, x, n);
+    }
+    return x;
+}
+
+template <int L>
+__global__ void __launch_bounds__(128)
+k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
+         const uint4* __restrict__ part, const Deficit* __restrict__ defs, const IterItem* __restrict__ iitems,
+         const uint4* __restrict__ ipart, uint32_t row_begin, uint32_t nrows, int full,
+         RowOut* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const uint32_t row = row_begin + i;
+    const RowInfo ri = info[row];
+    const Bucket bk = buckets[ri.bucket];
+    const RowMod m = mods[row];
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    const uint32_t ninv = m.ninv;
+    const uint32_t rl = row - bk.row_begin;
+
+    // combine split partials
+    Res<L> X;
+    set_small<L>(X, 1);
+    u128 def = 0;
+    for (uint32_t s = 0; s < bk.nsplit; ++s) {
+        const uint4 v = part[bk.part_base + (uint64_t)s * bk.nrows + rl];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, ninv);
+        const Deficit d = defs[bk.def_base + s];
+        def += ((u128)d.hi << 64 | d.lo) + 32 * L;
+    }
+    // the consecutive-integer tail
+    for (uint32_t k = 0; k < ri.it_count; ++k) {
+        const uint32_t idx = ri.it_begin + k;
+        const uint4 v = ipart[idx];
+        const IterItem it = iitems[idx];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, ninv);
+        const bool small = it.start + it.len - 1 < 0x80000000ull;
+        def += (u128)it.len * (small ? 32 : 64) + 32 * L;
+    }
+    // R mod n (Montgomery one), 2R mod n, R^2 mod n by doubling
+    Res<L> one;
+    set_small<L>(one, 1);
+    for (int k = 0; k < 32 * L; ++k) dbl_mod<L>(one, n);
+    Res<L> two = one;
+    dbl_mod<L>(two, n);
+    Res<L> R2 = one;
+    for (int k = 0; k < 32 * L; ++k) dbl_mod<L>(R2, n);
+    // X * 2^def: multiply by Mont(2^def) = (2R)^def in the Montgomery domain
+    const Res<L> Z = mont_pow<L>(two, def, one, n, ninv);
+    Res<L> V = mont_mul<L>(X, Z, n, ninv);
+    reduce_full<L>(V, n);                                   // V = value mod n
+
+    RowOut o;
+    o.pad = 0;
+    digits_base_p<L>(V, ri.p, &o.s0, &o.s1);
+    o.rem = 0;
+    o.quot = 0;
+    o.status = 0;
+    if (full) {
+        const uint64_t p = ri.p;
+        const Res<L> M = mont_mul<L>(V, R2, n, ninv);     // Montgomery form of T_p!
+        Res<L> mp;
+        set_small<L>(mp, p);
+        mp = mont_mul<L>(mp, R2, n, ninv);
+        const Res<L> two_p = mont_pow<L>(two, (u128)p, one, n, ninv);   // 2^p
+        Res<L> W;
+        bool ok = true;
+        if (ri.type == 0) {
+            int64_t cc = 0, uu = 0;
+            ok = find_cu(p, &cc, &uu);
+            const Res<L> mu = mont_of_signed<L>(uu, R2, n, ninv);
+            const Res<L> mc = mont_of_signed<L>(cc, R2, n, ninv);
+            W = mont_pow<L>(M, 6, one, n, ninv);                           // T!^6
+            Res<L> a = sub_mod2n<L>(two_p, one, n);                         // 2^p - 1
+            Res<L> u3 = mont_mul<L>(mont_mul<L>(mu, mu, n, ninv), mu, n, ninv);
+            Res<L> z;
+            set_small<L>(z, 0);
+            Res<L> b = sub_mod2n<L>(z, u3, n);                              // -u^3
+            a = mont_mul<L>(b, a, n, ninv);
+            Res<L> three;
+            set_small<L>(three, 3);
+            three = mont_mul<L>(three, R2, n, ninv);
+            b = mont_mul<L>(three, mont_mul<L>(mp, mu, n, ninv), n, ninv);  // 3pu
+            a = add_mod2n<L>(a, b, n);
+            W = mont_mul<L>(W, a, n, ninv);
+            // p/c - c with c^-1 = c^(p(p-1)-1) mod p^2
+            const u128 einv = (u128)p * (p - 1) - 1;
+            const Res<L> ci = mont_pow<L>(mc, einv, one, n, ninv);
+            a = sub_mod2n<L>(mont_mul<L>(mp, ci, n, ninv), mc, n);
+            W = mont_mul<L>(W, a, n, ninv);
+            // (3^p - 1)/2
+            a = sub_mod2n<L>(mont_pow<L>(three, (u128)p, one, n, ninv), one, n);
+            const Res<L> two_inv = mont_pow<L>(two, einv, one, n, ninv);
+            a = mont_mul<L>(a, two_inv, n, ninv);
+            W = mont_mul<L>(W, a, n, ninv);
+        } else if (ri.type == 1) {
+            int64_t aa = 0;
+            ok = find_a(p, &aa);
+            const Res<L> ma = mont_of_signed<L>(aa, R2, n, ninv);
+            W = mont_pow<L>(M, 4, one, n, ninv);                           // T!^4
+            Res<L> three, four;
+            set_small<L>(three, 3);
+            set_small<L>(four, 4);
+            three = mont_mul<L>(three, R2, n, ninv);
+            four = mont_mul<L>(four, R2, n, ninv);
+            Res<L> a = sub_mod2n<L>(mont_mul<L>(three, two_p, n, ninv), four, n);   // 3*2^p - 4
+            W = mont_mul<L>(W, a, n, ninv);
+            a = sub_mod2n<L>(mont_mul<L>(two, mont_mul<L>(ma, ma, n, ninv), n, ninv), mp, n);  // 2a^2 - p
+            W = mont_mul<L>(W, a, n, ninv);
+        } else {
+            W = mont_mul<L>(M, M, n, ninv);                                 // T!^2
+            W = mont_mul<L>(W, sub_mod2n<L>(one, two_p, n), n, ninv);      // (1 - 2^p)
+        }
+        Res<L> rawone;
+        set_small<L>(rawone, 1);
+        Res<L> Wv = mont_mul<L>(W, rawone, n, ninv);                       // out of Montgomery form
+        reduce_full<L>(Wv, n);
+        // + 1 mod n
+        add_limbs<L>(Wv, rawone.w);
+        if (geq<L>(Wv, n)) sub_limbs<L>(Wv, n);
+        uint64_t rem, quot;
+        digits_base_p<L>(Wv, p, &rem, &quot);
+        o.rem = rem;
+        o.quot = quot;
+        if (!ok) o.status = 2;              // representation not found
+        else if (rem != 0) o.status = 1;    // Wilson quotient check failed
+    }
+    out[row] = o;
+}
+
+// ===========================================================================
+// launch wrappers
+// ===========================================================================
+
+void launch_sieve_segments(uint32_t seg0, uint32_t nseg, uint64_t limit, const uint32_t* base, uint32_t nbase,
+                           uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st) {
+    if (!nseg) return;
+    k_sieve_segments<<<nseg, SIEVE_THREADS, 0, st>>>(seg0, limit, base, nbase, bitmap, seg_count);
+}
+void launch_scan_counts(const uint32_t* counts, uint32_t n, uint64_t first, uint64_t* offsets, cudaStream_t st) {
+    k_scan_counts<<<1, 1024, 0, st>>>(counts, n, first, offsets);
+}
+void launch_compact(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets,
+                    uint32_t* out32, uint64_t* out64, cudaStream_t st) {
+    if (!nseg) return;
+    k_compact<<<nseg, COMPACT_THREADS, 0, st>>>(lo0, SEG_SPAN, bitmap, offsets, out32, out64);
+}
+void launch_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t* bitmap,
+                          uint32_t* seg_count, cudaStream_t st) {
+    if (!nseg) return;
+    const uint64_t nbits = (uint64_t)nseg * SEG_BITS;
+    k_window_primes<<<(unsigned)(nbits / 256), 256, 0, st>>>(lo0, lo, hi, bitmap, seg_count);
+}
+void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys, uint64_t* out,
+                      cudaStream_t st) {
+    if (!nkeys) return;
+    k_count_leq<<<(nkeys + 127) / 128, 128, 0, st>>>(cols, ncols, keys, nkeys, out);
+}
+void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st) {
+    if (!nrows) return;
+    k_setup_rows<<<(nrows + 255) / 256, 256, 0, st>>>(info, nrows, mods);
+}
+void launch_sweep(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
+                  const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+    if (!nitems) return;
+#define WL_SWEEP(LL, RR) k_sweep<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs)
+    if (L == 2) { if (rpt == 2) WL_SWEEP(2, 2); else WL_SWEEP(2, 1); }
+    else if (L == 3) { if (rpt == 2) WL_SWEEP(3, 2); else WL_SWEEP(3, 1); }
+    else { if (rpt == 2) WL_SWEEP(4, 2); else WL_SWEEP(4, 1); }
+#undef WL_SWEEP
+}
+void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out, cudaStream_t st) {
+    if (!nitems) return;
+    const unsigned g = (nitems + 255) / 256;
+    if (L == 2) k_iterate<2><<<g, 256, 0, st>>>(items, nitems, mods, out);
+    else if (L == 3) k_iterate<3><<<g, 256, 0, st>>>(items, nitems, mods, out);
+    else k_iterate<4><<<g, 256, 0, st>>>(items, nitems, mods, out);
+}
+void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                   const Deficit* defs, const IterItem* iitems, const uint4* ipart, uint32_t row_begin,
+                   uint32_t nrows, int full, RowOut* out, cudaStream_t st) {
+    if (!nrows) return;
+    const unsigned g = (nrows + 127) / 128;
+    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
+    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
+    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
+}
+
+}  // namespace wl

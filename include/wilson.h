@@ -1,0 +1,141 @@
+/*
+ * wilson.h -- C ABI of the B200 Wilson-prime engine (libwilson.so).
+ *
+ * For every prime p in [pmin, pmax) the engine computes (p-1)! mod p^2 by the
+ * three-class reduction of mfl0p/CLWilson and reports the Wilson quotient
+ * w_p = ((p-1)! + 1)/p mod p, the results.txt lines and the checksum, bit for
+ * bit as the reference does.
+ *
+ * Conventions: plain C types only; caller-owned host buffers; library-owned
+ * device memory; every call returns 0 or a negative WL_ERR_* code (no exit()).
+ * A context belongs to one GPU and one host thread at a time.
+ *
+ * Which reference interface each entry point replaces (paths inside the
+ * reference project):
+ *   wl_open / wl_close    OpenCL platform, context and queue setup and the
+ *                         kernel builds (main.cpp:192-239, cl_wilson.cpp:1473-1485),
+ *                         cleanup (cl_wilson.cpp:84-107)
+ *   wl_search             one search run, cl_wilson() (cl_wilson.cpp:1442-1974,
+ *                         declared cl_wilson.h:72): test primes, class targets,
+ *                         the column sweep, iterate, getResults/processResult and
+ *                         finalizeResults' checksum
+ *   wl_rows               the per-prime residues the reference reads back before
+ *                         finalising (getDataFromGPU, cl_wilson.cpp:320-350) plus
+ *                         the per-prime quotient of processResult (691-900)
+ *   wl_batch              many ranges in one device pass (no counterpart: the
+ *                         reference runs one range per process)
+ *   wl_parse_uint64       the CLI number parser parse_uint64 (putil.c:34-116)
+ *   wl_check_range        setupSearch's range rules (cl_wilson.cpp:1146-1181,
+ *                         main.cpp:50-56)
+ */
+#ifndef WILSON_H
+#define WILSON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define WL_OK                 0
+#define WL_ERR_ARG          (-1)   /* bad argument / range rule violated */
+#define WL_ERR_CUDA         (-2)   /* CUDA runtime error */
+#define WL_ERR_NOPRIMES     (-3)   /* no primes in the range (cl_wilson.cpp:1532-1536) */
+#define WL_ERR_UNSUPPORTED  (-4)   /* configuration not supported by this build */
+#define WL_ERR_WILSON_CHECK (-5)   /* rem != 0 after the lift (cl_wilson.cpp:866-870) */
+#define WL_ERR_NO_REPR      (-6)   /* a, c or u not found (cl_wilson.cpp:554-558) */
+#define WL_ERR_CAPACITY     (-7)   /* caller buffer too small; *_needed tells the size */
+#define WL_ERR_NOMEM        (-8)   /* device allocation failed */
+
+/* reference limits (cl_wilson.h:8, cl_wilson.cpp:1162) */
+#define WL_MAXP      4611686018427387903ULL   /* (2^64-1)/4 */
+#define WL_MAX_WIDTH 10000000ULL
+
+typedef struct wl_ctx wl_ctx;
+
+/* one results.txt line: value 0 = Wilson prime, else Near-Wilson +-value */
+typedef struct {
+    uint64_t p;
+    int32_t value;
+    uint32_t pad;
+} wl_result;
+
+/* per-test-prime output */
+typedef struct {
+    uint64_t p;
+    uint64_t s0, s1;    /* T_p! mod p^2 = s0 + p*s1, T_p = (p-1)/6, /4 or /2;
+                           capped runs: the partial product over q < q_cap */
+    uint64_t rem, quot; /* ((p-1)! + 1) mod p^2 = rem + p*quot (full runs) */
+    uint32_t type;      /* 0: p = 1 mod 3, 1: p = 5 mod 12, 2: p = 11 mod 12 */
+    uint32_t status;    /* 0 ok, 1 rem != 0, 2 no representation */
+} wl_row;
+
+typedef struct {
+    uint64_t pmin, pmax;
+} wl_range;
+
+typedef struct {
+    uint64_t tested;        /* test primes in the range */
+    uint64_t checksum;      /* full: sum p + rem + quot; capped: sum p + s0 + s1 (mod 2^64) */
+    uint64_t targets[3];    /* class targets (0 if the class is empty) */
+    uint32_t results;       /* result lines */
+    uint32_t status;        /* 0 ok, else the first nonzero row status */
+} wl_range_result;
+
+typedef struct {
+    uint64_t tested;            /* test primes */
+    uint64_t per_class[3];      /* test primes per class */
+    uint64_t targets[3];        /* class targets of the (first) range */
+    uint64_t pi_maxtarget;      /* sieving primes <= the largest class target (first range) */
+    uint64_t cells;             /* column multiplications: sum over rows of its columns */
+    uint64_t tail_steps;        /* consecutive-integer multiplications */
+    uint64_t checksum;          /* as wl_range_result.checksum, summed over ranges */
+    uint32_t results;           /* result lines */
+    uint32_t kernel_launches;   /* CUDA kernels launched by the call */
+    double ms_device;           /* device time of the whole call (CUDA events) */
+    double ms_primes;           /* test-prime generation */
+    double ms_sieve;            /* column sieve (0 when the cache already covered it) */
+    double ms_sweep;            /* column sweep kernels */
+    double ms_iterate;          /* consecutive-integer tail */
+    double ms_finish;           /* combine + lift */
+    uint64_t h2d_bytes, d2h_bytes;
+} wl_stats;
+
+/* Open a context on CUDA device `device`. */
+int wl_open(int device, wl_ctx **out);
+void wl_close(wl_ctx *ctx);
+const char *wl_strerror(int code);
+/* The CUDA stream all work of the context is issued on (a cudaStream_t). */
+void *wl_stream(wl_ctx *ctx);
+
+/* Range rules of the reference: 5 <= pmin < pmax <= WL_MAXP, pmax - pmin <= WL_MAX_WIDTH. */
+int wl_check_range(uint64_t pmin, uint64_t pmax);
+
+/* Search [pmin, pmax).  q_cap = 0: full search.  q_cap > 0: capped sweep over
+ * sieving primes q < q_cap only (partial products; no tail, no lift, no
+ * result lines).  Result lines go to `results` in ascending p (up to `cap`;
+ * WL_ERR_CAPACITY when more exist, with stats->results set). */
+int wl_search(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_cap,
+              wl_result *results, size_t cap, wl_stats *stats);
+
+/* As wl_search, returning every test prime's row (ascending p). */
+int wl_rows(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_cap,
+            wl_row *rows, size_t cap, size_t *nrows, wl_stats *stats);
+
+/* Many ranges in one pass; out[i] describes ranges[i].  Result lines of all
+ * ranges are appended to `results` (ascending p within each range, ranges in
+ * order) when results != NULL. */
+int wl_batch(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap,
+             wl_range_result *out, wl_result *results, size_t cap, size_t *nresults,
+             wl_stats *stats);
+
+/* parse_uint64 of the reference CLI: returns 0, -1 (cannot parse) or -2 (out of range). */
+int wl_parse_uint64(uint64_t *result, const char *str, uint64_t lo, uint64_t hi);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WILSON_H */

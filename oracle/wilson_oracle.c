@@ -1,0 +1,689 @@
+/*
+ * wilson_oracle.c -- CPU restatement of mfl0p/CLWilson's Wilson-prime search.
+ *
+ * TEST INFRASTRUCTURE, NOT PRODUCT CODE.  This file is the checker for the CUDA
+ * engine in clwilson_b200/csrc.  Only tests/, __graft_entry__.smoke() and
+ * bench.py (its cpu_baseline / --impl reference legs) load the library built
+ * from it, and only to compare against or to time the reference algorithm on
+ * host cores.  The engine never calls it.
+ *
+ * Parity is pinned by: the reference's self-test known answers (cl_wilson.cpp
+ * 2076-2081: range [200,564), 57 lines, checksum 00000000000080A3; 2093-2098:
+ * range [86000000,87467200), checksum 0000097C61AB0943), the Wilson primes
+ * 5, 13, 563, and direct (p-1)! mod p^2 computed by exact integer arithmetic
+ * (tests/golden/make_golden.py).
+ *
+ * What is restated, and from where (paths are inside the reference project):
+ *   - 2-digit base-p Montgomery arithmetic modulo p^2 with R = 2^64
+ *       kernels/common.cl:16-260  (add_wide, mul_wide, invert, add/sub_mod[_c],
+ *       m2p_one, m2p_dup, m2p_add, m2p_square, m2p_mul, m2p_mul_r2, m2p_get)
+ *   - per-test-prime constants                       kernels/setup.cl:18-49
+ *   - test-prime classification and shared targets   cl_wilson.cpp:1549-1586
+ *   - Legendre exponents and equal-exponent packing  cl_wilson.cpp:1293-1365
+ *   - prime-power product into the residue           kernels/mulsmall.cl:32-58
+ *   - consecutive-integer tail + REDC out            kernels/iterate.cl:30-58
+ *   - representation search (a, c, u)                kernels/find.cl:14-117,
+ *                                                    cl_wilson.cpp:587-654
+ *   - class lift, +1, quotient/remainder             cl_wilson.cpp:731-870
+ *     (the reference uses GMP mpz; every step is a ring operation mod p^2, so
+ *      it is restated here in the same m2p arithmetic, value for value)
+ * The reference obtains primes from the third-party primesieve 12.3 library
+ * (cl_wilson.cpp:1529, 1316-1324); here test primes come from a deterministic
+ * Miller-Rabin test and sieving primes from a plain sieve of Eratosthenes.
+ * The find kernels' brute force is O(sqrt p) per prime; the driver uses
+ * Cornacchia's algorithm instead and the tests check both agree.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef uint64_t u64;
+typedef uint32_t u32;
+typedef unsigned __int128 u128;
+
+typedef struct { u64 s0, s1; } u64x2;
+
+/* ---------------- kernels/common.cl:16-113 ---------------- */
+
+static inline u64x2 mul_wide(u64 a, u64 b) {
+    u128 r = (u128)a * b;
+    u64x2 o = { (u64)r, (u64)(r >> 64) };
+    return o;
+}
+static inline u64 mul_hi(u64 a, u64 b) { return (u64)(((u128)a * b) >> 64); }
+static inline u64x2 add_wide(u64x2 a, u64x2 b) {
+    u64x2 r;
+    r.s0 = a.s0 + b.s0;
+    r.s1 = a.s1 + b.s1 + (r.s0 < a.s0 ? 1 : 0);
+    return r;
+}
+static inline int is_less_than(u64x2 a, u64x2 b) {
+    return (a.s1 < b.s1) || ((a.s1 == b.s1) && (a.s0 < b.s0));
+}
+/* p * p_inv = 1 (mod 2^64), Newton iteration (common.cl:76-81) */
+static u64 invert(u64 p) {
+    u64 p_inv = 1, prev = 0;
+    while (p_inv != prev) { prev = p_inv; p_inv *= 2 - p * p_inv; }
+    return p_inv;
+}
+static inline u64 add_mod(u64 x, u64 y, u64 p) { u64 cp = (x >= p - y) ? p : 0; return x + y - cp; }
+static inline u64 add_mod_c(u64 x, u64 y, u64 p, u64 *c) {
+    int carry = (x >= p - y); *c = carry ? 1 : 0; return x + y - (carry ? p : 0);
+}
+static inline u64 sub_mod(u64 x, u64 y, u64 p) { u64 cp = (x < y) ? p : 0; return x - y + cp; }
+static inline u64 sub_mod_c(u64 x, u64 y, u64 p, u64 *c) {
+    int carry = (x < y); *c = carry ? 1 : 0; return x - y + (carry ? p : 0);
+}
+
+/* ---------------- kernels/common.cl:115-260 (m2p_*) ---------------- */
+
+/* 2^64 mod p^2 = Montgomery form of 1 (common.cl:120-130) */
+static u64x2 m2p_one(u64 p) {
+    if ((p >> 32) == 0) {
+        u64 p2 = p * p, r_p2 = (0 - p2) % p2;
+        u64x2 o = { r_p2 % p, r_p2 / p };
+        return o;
+    }
+    u64 mp = 0 - p;
+    u64x2 o = { mp % p, mp / p + 1 };
+    return o;
+}
+static inline u64x2 m2p_dup(u64x2 x, u64 p) {
+    u64 c; u64 l = add_mod_c(x.s0, x.s0, p, &c); u64 h = add_mod(x.s1 + c, x.s1, p);
+    u64x2 o = { l, h }; return o;
+}
+static inline u64x2 m2p_add(u64x2 x, u64x2 y, u64 p) {
+    u64 c; u64 l = add_mod_c(x.s0, y.s0, p, &c); u64 h = add_mod(x.s1 + c, y.s1, p);
+    u64x2 o = { l, h }; return o;
+}
+/* subtraction with the same digit conventions (the mirror of m2p_add; the
+   reference performs its subtractions in GMP, cl_wilson.cpp:757-820) */
+static inline u64x2 m2p_sub(u64x2 x, u64x2 y, u64 p) {
+    u64 c; u64 l = sub_mod_c(x.s0, y.s0, p, &c); u64 h = sub_mod(x.s1, y.s1 + c, p);
+    u64x2 o = { l, h }; return o;
+}
+static inline u64x2 m2p_square(u64x2 x, u64 p, u64 q) {
+    const u64x2 t = mul_wide(x.s0, x.s0);
+    const u64 u0 = q * t.s0;
+    const u64 t1 = t.s1;
+    const u64 v1 = mul_hi(p, u0);
+    const u64x2 x01 = mul_wide(x.s0, x.s1);
+    u64x2 u0w = { u0, 0 };
+    const u64x2 x01u = add_wide(x01, u0w);
+    const u64x2 tp = add_wide(x01u, x01); int tp_carry = is_less_than(tp, x01);
+    const u64 tp_h = tp.s1, tpc = (tp_carry | (tp_h >= p)) ? p : 0;
+    const u64 up0 = q * tp.s0;
+    const u64 t1p = tp_h - tpc;
+    const u64 v1p = mul_hi(p, up0);
+    u64 c;
+    const u64 z0 = sub_mod_c(t1, v1, p, &c);
+    const u64 z1 = sub_mod(t1p, v1p + c, p);
+    u64x2 o = { z0, z1 }; return o;
+}
+static inline u64x2 m2p_mul(u64x2 x, u64x2 y, u64 p, u64 q) {
+    const u64x2 t = mul_wide(x.s0, y.s0);
+    const u64 u0 = q * t.s0;
+    const u64 t1 = t.s1;
+    const u64 v1 = mul_hi(p, u0);
+    u64x2 u0w = { u0, 0 };
+    const u64x2 x0y1u = add_wide(mul_wide(x.s0, y.s1), u0w);
+    const u64x2 x1y0 = mul_wide(x.s1, y.s0);
+    const u64x2 tp = add_wide(x0y1u, x1y0); int tp_carry = is_less_than(tp, x1y0);
+    const u64 tp_h = tp.s1, tpc = (tp_carry | (tp_h >= p)) ? p : 0;
+    const u64 up0 = q * tp.s0;
+    const u64 t1p = tp_h - tpc;
+    const u64 v1p = mul_hi(p, up0);
+    u64 c;
+    const u64 z0 = sub_mod_c(t1, v1, p, &c);
+    const u64 z1 = sub_mod(t1p, v1p + c, p);
+    u64x2 o = { z0, z1 }; return o;
+}
+/* one 64-bit word times a residue (common.cl:217-243); with y = R^2 mod p^2
+   this converts x < 2^64 into Montgomery form */
+static inline u64x2 m2p_mul_r2(u64 x, u64x2 y, u64 p, u64 q) {
+    const u64x2 t = mul_wide(x, y.s0);
+    const u64 u0 = q * t.s0;
+    const u64 t1 = t.s1;
+    const u64 v1 = mul_hi(p, u0);
+    u64x2 u0w = { u0, 0 };
+    const u64x2 tp = add_wide(mul_wide(x, y.s1), u0w);
+    const u64 tp_h = tp.s1, tpc = (tp_h >= p) ? p : 0;
+    const u64 up0 = q * tp.s0;
+    const u64 t1p = tp_h - tpc;
+    const u64 v1p = mul_hi(p, up0);
+    u64 c;
+    const u64 z0 = sub_mod_c(t1, v1, p, &c);
+    const u64 z1 = sub_mod(t1p, v1p + c, p);
+    u64x2 o = { z0, z1 }; return o;
+}
+/* REDC out of Montgomery form (common.cl:246-260) */
+static inline u64x2 m2p_get(u64x2 x, u64 p, u64 q) {
+    const u64 u0 = q * x.s0;
+    const u64 v1 = mul_hi(p, u0);
+    const u64 tp = x.s1 + u0;
+    const u64 up0 = q * tp;
+    const u64 t1p = (tp < x.s1) ? 1 : 0;
+    const u64 v1p = mul_hi(p, up0);
+    u64 c;
+    const u64 z0 = sub_mod_c(0, v1, p, &c);
+    const u64 z1 = sub_mod(t1p, v1p + c, p);
+    u64x2 o = { z0, z1 }; return o;
+}
+
+/* ---------------- per-test-prime constants (setup.cl:18-45) ---------------- */
+
+typedef struct { u64 p, q; u64x2 one, r2; } tpconst;
+
+static tpconst setup_prime(u64 p) {
+    tpconst c;
+    c.p = p;
+    c.q = invert(p);
+    c.one = m2p_one(p);
+    u64x2 two = m2p_dup(c.one, p);
+    u64x2 r2 = m2p_dup(two, p);
+    for (int i = 0; i < 5; ++i) r2 = m2p_square(r2, p, c.q);   /* 4^(2^5) = 2^64 */
+    c.r2 = r2;
+    return c;
+}
+static inline u64x2 to_mont(const tpconst *c, u64 x) { return m2p_mul_r2(x, c->r2, c->p, c->q); }
+
+static u64x2 m2p_pow(const tpconst *c, u64x2 base, u128 e) {
+    u64x2 r = c->one;
+    int top = 127;
+    while (top >= 0 && !((e >> top) & 1)) --top;
+    for (int b = top; b >= 0; --b) {
+        r = m2p_square(r, c->p, c->q);
+        if ((e >> b) & 1) r = m2p_mul(r, base, c->p, c->q);
+    }
+    return r;
+}
+/* x^-1 mod p^2 = x^(p(p-1)-1) for x coprime to p (the reference calls mpz_invert) */
+static u64x2 m2p_inv(const tpconst *c, u64x2 x) {
+    u128 e = (u128)c->p * (c->p - 1) - 1;
+    return m2p_pow(c, x, e);
+}
+static u64x2 mont_signed(const tpconst *c, int64_t v) {
+    u64x2 m = to_mont(c, (u64)(v < 0 ? -v : v));
+    if (v < 0) { u64x2 z = { 0, 0 }; m = m2p_sub(z, m, c->p); }
+    return m;
+}
+
+/* ---------------- representation search ---------------- */
+
+/* integer square root, digit by digit (find.cl:14-43) */
+u64 orc_isqrt(u64 n) {
+    u64 x = n, c = 0, d = 1ULL << 62;
+    while (d > n) d >>= 2;
+    while (d != 0) {
+        if (x >= c + d) { x -= c + d; c = (c >> 1) + d; }
+        else c >>= 1;
+        d >>= 2;
+    }
+    return c;
+}
+
+/* brute-force searches as in find.cl (finda 46-68, findc 71-92, findu 95-117)
+   with the host's bounds and sign rules (cl_wilson.cpp:587-654).  The serial
+   loop returns the smallest admissible loop index. */
+int orc_find_a_brute(u64 p, int64_t *out) {
+    u64 maxa = orc_isqrt(p);
+    for (u64 a = 1; a <= maxa; a += 2) {
+        u64 b2 = p - a * a, b = orc_isqrt(b2);
+        if (b * b == b2) { *out = (a % 4 == 3) ? -(int64_t)a : (int64_t)a; return 0; }
+    }
+    return -1;
+}
+int orc_find_c_brute(u64 p, int64_t *out) {
+    u64 p4 = 4 * p, maxd = orc_isqrt(p4 / 27);
+    for (u64 d = 1; d <= maxd + 1; ++d) {
+        if (27 * d * d > p4) break;
+        u64 c2 = p4 - 27 * d * d, c = orc_isqrt(c2);
+        if (c * c == c2) { *out = (c % 3 == 2) ? -(int64_t)c : (int64_t)c; return 0; }
+    }
+    return -1;
+}
+int orc_find_u_brute(u64 p, int64_t *out) {
+    u64 p4 = 4 * p, maxv = orc_isqrt(p4 / 3);
+    u32 umod = (((p - 1) / 6) % 2 == 0) ? 1 : 2;
+    for (u64 v = 1; v <= maxv + 1; ++v) {
+        if (3 * v * v > p4) break;
+        u64 u2 = p4 - 3 * v * v, u = orc_isqrt(u2);
+        if (u * u == u2) { *out = (u % 3 == umod) ? (int64_t)u : -(int64_t)u; return 0; }
+    }
+    return -1;
+}
+
+/* arithmetic modulo p (< 2^62) for Cornacchia */
+static inline u64 mulmod64(u64 a, u64 b, u64 m) { return (u64)(((u128)a * b) % m); }
+static u64 powmod64(u64 b, u64 e, u64 m) {
+    u64 r = 1 % m; b %= m;
+    while (e) { if (e & 1) r = mulmod64(r, b, m); b = mulmod64(b, b, m); e >>= 1; }
+    return r;
+}
+/* Cornacchia: x^2 + d*y^2 = p from r0^2 = -d (mod p); returns x */
+static int cornacchia(u64 p, u64 d, u64 r0, u64 *x, u64 *y) {
+    if (r0 <= p / 2) r0 = p - r0;       /* use the root in (p/2, p) */
+    u64 a = p, b = r0, lim = orc_isqrt(p);
+    while (b > lim) { u64 t = a % b; a = b; b = t; }
+    u64 rest = p - b * b;
+    if (rest % d) return -1;
+    u64 yy = rest / d, yr = orc_isqrt(yy);
+    if (yr * yr != yy) return -1;
+    *x = b; *y = yr;
+    return 0;
+}
+/* a with p = a^2 + b^2, a = 1 (mod 4), for p = 1 (mod 4) */
+int orc_cornacchia_a(u64 p, int64_t *out) {
+    for (u64 g = 2; g < 1000; ++g) {
+        if (powmod64(g, (p - 1) / 2, p) != p - 1) continue;   /* g non-residue */
+        u64 r = powmod64(g, (p - 1) / 4, p), x, y;             /* r^2 = -1 */
+        if (cornacchia(p, 1, r, &x, &y)) return -1;
+        u64 a = (x & 1) ? x : y;
+        *out = (a % 4 == 3) ? -(int64_t)a : (int64_t)a;
+        return 0;
+    }
+    return -1;
+}
+/* c with 4p = c^2 + 27 d^2 (c = 1 mod 3) and one u with 4p = u^2 + 3 v^2
+   (u = umod mod 3), for p = 1 (mod 3) */
+int orc_cornacchia_cu(u64 p, int64_t *c_out, int64_t *u_out) {
+    for (u64 g = 2; g < 1000; ++g) {
+        u64 w = powmod64(g, (p - 1) / 3, p);                   /* cube root of 1 */
+        if (w == 1) continue;
+        u64 r = (2 * w + 1) % p;                               /* r^2 = -3 */
+        u64 x, y;
+        if (cornacchia(p, 3, r, &x, &y)) return -1;
+        /* 4p = (2x)^2 + 3(2y)^2 = (x+3y)^2 + 3(x-y)^2 = (x-3y)^2 + 3(x+y)^2 */
+        int64_t X = (int64_t)x, Y = (int64_t)y;
+        int64_t us[3] = { 2 * X, X + 3 * Y, X - 3 * Y };
+        int64_t vs[3] = { 2 * Y, X - Y, X + Y };
+        u32 umod = (((p - 1) / 6) % 2 == 0) ? 1 : 2;
+        u64 u = (u64)(us[0] < 0 ? -us[0] : us[0]);
+        *u_out = (u % 3 == umod) ? (int64_t)u : -(int64_t)u;
+        for (int k = 0; k < 3; ++k) {
+            int64_t v = vs[k] < 0 ? -vs[k] : vs[k];
+            if (v % 3 == 0) {
+                u64 c = (u64)(us[k] < 0 ? -us[k] : us[k]);
+                *c_out = (c % 3 == 2) ? -(int64_t)c : (int64_t)c;
+                return 0;
+            }
+        }
+        return -1;
+    }
+    return -1;
+}
+
+/* ---------------- class lift (cl_wilson.cpp:731-870) ---------------- */
+
+/* res: Montgomery form of T_p! mod p^2.  Returns 0 and (rem, quot) of
+   ((p-1)! + 1) mod p^2 = rem + p*quot, or -1 if no representation was found. */
+static int lift(const tpconst *c, u32 type, u64x2 res, u64 *rem, u64 *quot) {
+    const u64 p = c->p, q = c->q;
+    u64x2 W;
+    u64x2 m2 = to_mont(c, 2), mp = to_mont(c, p);
+    u64x2 two_p = m2p_pow(c, m2, p);                            /* 2^p mod p^2 */
+    if (type == 0) {
+        int64_t uu, cc;
+        if (orc_cornacchia_cu(p, &cc, &uu)) return -1;
+        u64x2 mu = mont_signed(c, uu), mc = mont_signed(c, cc);
+        W = m2p_pow(c, res, 6);                                 /* T!^6 */
+        u64x2 a = m2p_sub(two_p, c->one, p);                    /* 2^p - 1 */
+        u64x2 u3 = m2p_mul(m2p_square(mu, p, q), mu, p, q);
+        u64x2 z = { 0, 0 };
+        u64x2 b = m2p_sub(z, u3, p);                            /* -u^3 */
+        a = m2p_mul(b, a, p, q);
+        b = m2p_mul(to_mont(c, 3), m2p_mul(mp, mu, p, q), p, q); /* 3pu */
+        a = m2p_add(a, b, p);
+        W = m2p_mul(W, a, p, q);
+        a = m2p_sub(m2p_mul(mp, m2p_inv(c, mc), p, q), mc, p); /* p/c - c */
+        W = m2p_mul(W, a, p, q);
+        a = m2p_sub(m2p_pow(c, to_mont(c, 3), p), c->one, p);   /* 3^p - 1 */
+        a = m2p_mul(a, m2p_inv(c, m2), p, q);                   /* /2 */
+        W = m2p_mul(W, a, p, q);
+    } else if (type == 1) {
+        int64_t aa;
+        if (orc_cornacchia_a(p, &aa)) return -1;
+        u64x2 ma = mont_signed(c, aa);
+        W = m2p_pow(c, res, 4);                                 /* T!^4 */
+        u64x2 a = m2p_sub(m2p_mul(to_mont(c, 3), two_p, p, q), to_mont(c, 4), p);
+        W = m2p_mul(W, a, p, q);                                /* (3*2^p - 4) */
+        a = m2p_sub(m2p_mul(m2, m2p_square(ma, p, q), p, q), mp, p);
+        W = m2p_mul(W, a, p, q);                                /* (2a^2 - p) */
+    } else {
+        W = m2p_square(res, p, q);                              /* T!^2 */
+        W = m2p_mul(W, m2p_sub(c->one, two_p, p), p, q);        /* (1 - 2^p) */
+    }
+    u64x2 v = m2p_get(W, p, q);                                 /* digits of W */
+    /* +1 mod p^2 (cl_wilson.cpp:858-862); the digits are rem and quot */
+    v.s0 += 1;
+    if (v.s0 == p) { v.s0 = 0; v.s1 += 1; if (v.s1 == p) v.s1 = 0; }
+    *rem = v.s0; *quot = v.s1;
+    return 0;
+}
+
+/* ---------------- primes ---------------- */
+
+static int is_prime_u64(u64 n) {
+    static const u32 small[] = { 2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71 };
+    if (n < 2) return 0;
+    for (unsigned i = 0; i < sizeof(small) / sizeof(small[0]); ++i) {
+        if (n == small[i]) return 1;
+        if (n % small[i] == 0) return 0;
+    }
+    /* deterministic Miller-Rabin for n < 2^64 (bases of J. Sinclair) */
+    static const u64 bases[] = { 2, 325, 9375, 28178, 450775, 9780504, 1795265022 };
+    u64 d = n - 1; int s = 0;
+    while (!(d & 1)) { d >>= 1; ++s; }
+    for (int i = 0; i < 7; ++i) {
+        u64 a = bases[i] % n;
+        if (a == 0) continue;
+        u64 x = powmod64(a, d, n);
+        if (x == 1 || x == n - 1) continue;
+        int ok = 0;
+        for (int r = 1; r < s; ++r) {
+            x = mulmod64(x, x, n);
+            if (x == n - 1) { ok = 1; break; }
+        }
+        if (!ok) return 0;
+    }
+    return 1;
+}
+int orc_is_prime(u64 n) { return is_prime_u64(n); }
+
+/* primes in [lo, hi) in ascending order; returns the count (writes at most cap) */
+size_t orc_list_primes(u64 lo, u64 hi, u64 *out, size_t cap) {
+    size_t n = 0;
+    for (u64 x = lo; x < hi; ++x) {
+        if (is_prime_u64(x)) { if (n < cap && out) out[n] = x; ++n; }
+    }
+    return n;
+}
+
+/* odd primes below sqrt(limit), then a segmented odd-only sieve of
+   Eratosthenes over [lo, hi) (limit <= 2^34) */
+typedef struct { u32 *p; size_t n; } sieve_base;
+
+static sieve_base make_base(u64 limit) {
+    sieve_base b = { NULL, 0 };
+    u64 r = 1;
+    while (r * r < limit) ++r;                 /* r >= sqrt(limit) */
+    uint8_t *comp = (uint8_t *)calloc(r + 2, 1);
+    b.p = (u32 *)malloc((r / 2 + 2) * sizeof(u32));
+    for (u64 i = 3; i <= r; i += 2) {
+        if (comp[i]) continue;
+        b.p[b.n++] = (u32)i;
+        for (u64 j = i * i; j <= r; j += 2 * i) comp[j] = 1;
+    }
+    free(comp);
+    return b;
+}
+
+/* primes in [lo, hi) in ascending order into out; returns the count */
+static size_t sieve_segment(const sieve_base *b, u64 lo, u64 hi, uint8_t *scratch, u32 *out) {
+    size_t n = 0;
+    if (lo <= 2 && 2 < hi) out[n++] = 2;
+    u64 first = lo | 1;                         /* first odd >= lo */
+    if (first >= hi) return n;
+    u64 nodd = (hi - first + 1) / 2;            /* odd numbers first, first+2, ... < hi */
+    memset(scratch, 0, nodd);
+    for (size_t k = 0; k < b->n; ++k) {
+        u64 q = b->p[k];
+        if (q * q >= hi) break;
+        u64 m = (first + q - 1) / q * q;
+        if (m < q * q) m = q * q;
+        if (!(m & 1)) m += q;
+        for (u64 j = (m - first) / 2; j < nodd; j += q) scratch[j] = 1;
+    }
+    for (u64 j = 0; j < nodd; ++j) {
+        u64 v = first + 2 * j;
+        if (!scratch[j] && v > 1) out[n++] = (u32)v;
+    }
+    return n;
+}
+
+#define SIEVE_CHUNK (1ULL << 24)
+
+size_t orc_count_primes_below(u64 limit) {
+    sieve_base b = make_base(limit);
+    uint8_t *scratch = (uint8_t *)malloc(SIEVE_CHUNK / 2 + 2);
+    u32 *buf = (u32 *)malloc((SIEVE_CHUNK / 2 + 2) * sizeof(u32));
+    size_t total = 0;
+    for (u64 lo = 0; lo < limit; lo += SIEVE_CHUNK) {
+        u64 hi = lo + SIEVE_CHUNK < limit ? lo + SIEVE_CHUNK : limit;
+        total += sieve_segment(&b, lo, hi, scratch, buf);
+    }
+    free(scratch); free(buf); free(b.p);
+    return total;
+}
+
+/* ---------------- column builder (cl_wilson.cpp:1293-1365) ---------------- */
+
+typedef struct { u64 prime, exp, curbit; } column;
+
+/* Legendre exponent of prime in target! and the bit below its top bit
+   (getPower, cl_wilson.cpp:1293-1313) */
+static void get_power(u64 prime, u64 target, u64 *exp, u64 *curbit) {
+    if (prime > target) { *exp = 0; *curbit = 0; return; }
+    u64 total = 0, cur = prime, q = target / cur;
+    while (q) {
+        total += q;
+        u128 pp = (u128)cur * prime;
+        if (pp > target) break;
+        cur = (u64)pp;
+        q = target / cur;
+    }
+    u64 cb = 0x8000000000000000ULL;
+    if (total > 1) cb >>= (__builtin_clzll(total) + 1);
+    *exp = total; *curbit = cb;
+}
+
+/* columns of one chunk of primes for one class target: primes q <= target and
+   q < qcap, runs of equal exponent multiplied together while the product fits
+   64 bits (get32bitprimes, cl_wilson.cpp:1330-1357) */
+static column *build_columns(const u32 *primes, size_t np, u64 target, u64 qcap, size_t *ncol) {
+    size_t lim = 0;
+    while (lim < np && primes[lim] <= target && (qcap == 0 || primes[lim] < qcap)) ++lim;
+    column *cols = (column *)malloc((lim + 1) * sizeof(column));
+    size_t m = 0;
+    if (lim) {
+        get_power(primes[0], target, &cols[0].exp, &cols[0].curbit);
+        cols[0].prime = primes[0];
+        m = 1;
+        for (size_t i = 1; i < lim; ++m) {
+            cols[m].prime = primes[i];
+            get_power(primes[i], target, &cols[m].exp, &cols[m].curbit);
+            for (++i; i < lim; ++i) {
+                u64 e, cb; get_power(primes[i], target, &e, &cb);
+                if (e != cols[m].exp) break;
+                u128 pp = (u128)cols[m].prime * primes[i];
+                if (pp > 0xFFFFFFFFFFFFFFFFULL) break;
+                cols[m].prime = (u64)pp;
+            }
+        }
+    }
+    *ncol = m;
+    return cols;
+}
+
+/* prime-power product of one column set into a residue (mulsmall.cl:32-58) */
+static u64x2 column_product(const tpconst *c, const column *cols, size_t ncol, u64x2 residue) {
+    for (size_t j = 0; j < ncol; ++j) {
+        const u64x2 base = to_mont(c, cols[j].prime);
+        u64x2 pp;
+        if (cols[j].exp == 1) pp = base;
+        else {
+            u64x2 a = base;
+            u64 cb = cols[j].curbit;
+            while (cb) {
+                a = m2p_square(a, c->p, c->q);
+                if (cols[j].exp & cb) a = m2p_mul(a, base, c->p, c->q);
+                cb >>= 1;
+            }
+            pp = a;
+        }
+        residue = m2p_mul(residue, pp, c->p, c->q);
+    }
+    return residue;
+}
+
+/* consecutive integers target_type+1 .. target_p (iterate.cl:30-58) */
+static u64x2 iterate_tail(const tpconst *c, u64 from_excl, u64 to_incl, u64x2 residue) {
+    u64x2 total = c->one;
+    if (from_excl < to_incl) {
+        u64x2 mn = to_mont(c, from_excl + 1);
+        for (u64 n = from_excl + 1; n <= to_incl; ++n) {
+            total = m2p_mul(mn, total, c->p, c->q);
+            mn = m2p_add(mn, c->one, c->p);
+        }
+    }
+    return m2p_mul(total, residue, c->p, c->q);
+}
+
+/* ---------------- search driver ---------------- */
+
+typedef struct {
+    u64 p;          /* test prime */
+    u64 s0, s1;     /* digits of T_p! mod p^2 (uncapped) or of the capped partial product */
+    u64 rem, quot;  /* ((p-1)! + 1) mod p^2 = rem + p*quot  (uncapped only) */
+    u32 type;       /* 0: p=1 mod 3, 1: p=5 mod 12, 2: p=11 mod 12 */
+    int32_t status; /* 0 ok, -1 representation not found, 1 capped (no lift) */
+} orc_row;
+
+/* class of p and its own target (cl_wilson.cpp:1552-1586) */
+static int classify(u64 p, u32 *type, u64 *target) {
+    if (p % 3 == 1) { *type = 0; *target = (p - 1) / 6; }
+    else if (p % 12 == 5) { *type = 1; *target = (p - 1) / 4; }
+    else if (p % 12 == 11) { *type = 2; *target = (p - 1) / 2; }
+    else return -1;
+    return 0;
+}
+
+/*
+ * Search every prime in [pmin, pmax).  qcap == 0: full search (T_p! and the
+ * lift).  qcap > 0: capped sweep, the partial product over sieving primes
+ * q < qcap (q <= the class target) with Legendre exponents of the class
+ * target; no iterate tail, no lift.  sel/nsel: optional subset of row indices
+ * (ascending) to compute; other rows are returned with status 2 and zeros.
+ * targets[3] receives the shared class targets (0 when a class is empty).
+ * Returns the number of test primes (rows written: min(count, cap)), or -1.
+ */
+long orc_search(u64 pmin, u64 pmax, u64 qcap, int threads, const u32 *sel, size_t nsel,
+                orc_row *out, size_t cap, u64 *targets) {
+    size_t ntp = orc_list_primes(pmin, pmax, NULL, 0);
+    u64 *tp = (u64 *)malloc((ntp + 1) * sizeof(u64));
+    orc_list_primes(pmin, pmax, tp, ntp);
+    u64 tt[3] = { 0, 0, 0 };
+    for (size_t i = 0; i < ntp; ++i) {
+        u32 t; u64 tg;
+        if (classify(tp[i], &t, &tg)) { free(tp); return -1; }
+        if (!tt[t]) tt[t] = tg;
+    }
+    if (targets) for (int t = 0; t < 3; ++t) targets[t] = tt[t];
+    u64 maxt = tt[0] > tt[1] ? tt[0] : tt[1]; if (tt[2] > maxt) maxt = tt[2];
+    u64 slimit = maxt + 1;
+    if (qcap && qcap < slimit) slimit = qcap;
+
+    unsigned char *want = NULL;
+    if (sel) {
+        want = (unsigned char *)calloc(ntp + 1, 1);
+        for (size_t i = 0; i < nsel; ++i) if (sel[i] < ntp) want[sel[i]] = 1;
+    }
+    size_t nw = ntp < cap ? ntp : cap;
+    tpconst *cs = (tpconst *)malloc((nw + 1) * sizeof(tpconst));
+    u64x2 *res = (u64x2 *)malloc((nw + 1) * sizeof(u64x2));
+    u32 *types = (u32 *)malloc((nw + 1) * sizeof(u32));
+    for (size_t i = 0; i < nw; ++i) {
+        u64 tg; classify(tp[i], &types[i], &tg);
+        cs[i] = setup_prime(tp[i]);
+        res[i] = cs[i].one;                                   /* setup.cl:47-49 */
+    }
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+    /* the column sweep, chunk by chunk as the reference's main loop
+       (cl_wilson.cpp:1856-1929) */
+    sieve_base base = make_base(slimit);
+    uint8_t *scratch = (uint8_t *)malloc(SIEVE_CHUNK / 2 + 2);
+    u32 *buf = (u32 *)malloc((SIEVE_CHUNK / 2 + 2) * sizeof(u32));
+    for (u64 lo = 0; lo < slimit; lo += SIEVE_CHUNK) {
+        u64 hi = lo + SIEVE_CHUNK < slimit ? lo + SIEVE_CHUNK : slimit;
+        size_t np = sieve_segment(&base, lo, hi, scratch, buf);
+        column *cols[3]; size_t ncol[3];
+        for (int t = 0; t < 3; ++t) cols[t] = build_columns(buf, np, tt[t], qcap, &ncol[t]);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+        for (long i = 0; i < (long)nw; ++i) {
+            if (want && !want[i]) continue;
+            u32 t = types[i];
+            res[i] = column_product(&cs[i], cols[t], ncol[t], res[i]);
+        }
+        for (int t = 0; t < 3; ++t) free(cols[t]);
+    }
+    free(scratch); free(buf); free(base.p);
+
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (long i = 0; i < (long)nw; ++i) {
+        orc_row *r = &out[i];
+        memset(r, 0, sizeof(*r));
+        u64 p = tp[i]; u32 t = 0; u64 tg = 0;
+        classify(p, &t, &tg);
+        r->p = p; r->type = t;
+        if (want && !want[i]) { r->status = 2; continue; }
+        const tpconst *c = &cs[i];
+        u64x2 rr = res[i];
+        if (qcap) {
+            u64x2 v = m2p_get(rr, c->p, c->q);
+            r->s0 = v.s0; r->s1 = v.s1; r->status = 1;
+            continue;
+        }
+        rr = iterate_tail(c, tt[t], tg, rr);                  /* iterate.cl:30-58 */
+        u64x2 v = m2p_get(rr, c->p, c->q);
+        r->s0 = v.s0; r->s1 = v.s1;
+        r->status = lift(c, t, rr, &r->rem, &r->quot);
+    }
+    free(cs); free(res); free(types);
+    free(want);
+    free(tp);
+    return (long)ntp;
+}
+
+/* (p-1)! mod p^2 by direct multiplication of 1..p-1 (small p only): digits */
+void orc_factorial_mod_p2(u64 p, u64 *s0, u64 *s1) {
+    tpconst c = setup_prime(p);
+    u64x2 r = iterate_tail(&c, 0, p - 1, c.one);
+    u64x2 v = m2p_get(r, c.p, c.q);
+    *s0 = v.s0; *s1 = v.s1;
+}
+
+/* T! mod p^2 by direct multiplication (small T only): digits */
+void orc_small_factorial(u64 p, u64 T, u64 *s0, u64 *s1) {
+    tpconst c = setup_prime(p);
+    u64x2 r = iterate_tail(&c, 0, T, c.one);
+    u64x2 v = m2p_get(r, c.p, c.q);
+    *s0 = v.s0; *s1 = v.s1;
+}
+
+/* the lift applied to given digits of T_p! (for unit tests of the lift alone) */
+int orc_lift_digits(u64 p, u64 s0, u64 s1, u64 *rem, u64 *quot) {
+    tpconst c = setup_prime(p);
+    u32 t; u64 tg;
+    if (classify(p, &t, &tg)) return -1;
+    /* Montgomery form of s0 + p*s1 */
+    u64x2 m = m2p_add(to_mont(&c, s0), m2p_mul(to_mont(&c, p), to_mont(&c, s1), c.p, c.q), c.p);
+    return lift(&c, t, m, rem, quot);
+}
+
+int orc_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

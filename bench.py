@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Wilson-prime search throughput on B200 (one JSON line on rank 0).
+
+Workloads (--workload):
+  plain-small   [default] every prime p in [1e9 + r*1e6, 1e9 + (r+1)*1e6) on rank r:
+                the full search of the reference's CPU-runnable configuration
+                ((p-1)! mod p^2, w_p, result lines, checksum), about 48k primes per GPU.
+  plain-mid     every prime in [1e13, 1e13 + 1e7): column sweep capped at q < 2^32
+                (the full run is about a day on one GPU); partial products per prime.
+  plain-top     every prime in [2^62-1-1e7, 2^62-1): column sweep capped at q < 2^32.
+  batched       256 ranges from numpy default_rng(0), log-uniform starts in
+                [1e8, 2^62-1e7) and widths in [1e3, 1e7], column sweep capped at q < 2^28.
+
+A step is one call of the engine's C ABI on the workload (test primes, columns,
+sweep, tail, lift, results).  `value` is device time (CUDA events on the
+engine's stream, L2 flushed between steps); `e2e` is host wall time around the
+same C-ABI call, which includes its host<->device copies.
+
+--impl reference times the reference algorithm on the host cores instead (the
+CPU restatement under oracle/, all threads) on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PLAIN_SMALL = (10**9, 10**6)
+OPS_PER_CELL = {2: 9, 3: 13, 4: 17}   # multiply-class PTX ops of one cell step (wl_arith.cuh)
+
+
+def limbs_for(pmax_incl: int) -> int:
+    return 2 if pmax_incl < 2**31 else (3 if pmax_incl < 2**47 else 4)
+
+
+def batched_ranges(seed: int = 0, n: int = 256):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(1e8), np.log(2.0**62 - 1e7)
+    starts = np.exp(rng.uniform(lo, hi, n))
+    widths = np.round(np.exp(rng.uniform(np.log(1e3), np.log(1e7), n)))
+    out = []
+    for s, w in zip(starts, widths):
+        a = int(s)
+        b = min(a + int(w), 2**62 - 1)
+        out.append((max(a, 5), b))
+    return out
+
+
+def workload(name: str, rank: int, world: int, width: int = PLAIN_SMALL[1]):
+    """(ranges, q_cap, description) for this rank."""
+    if name == "plain-small":
+        a = PLAIN_SMALL[0] + rank * width
+        return [(a, a + width)], 0, f"plain-small: every prime in [{a}, {a + width}), full search"
+    if name == "plain-mid":
+        a = 10**13 + rank * 10**7
+        return [(a, a + 10**7)], 2**32, f"plain-mid: every prime in [{a}, {a + 10**7}), columns q < 2^32"
+    if name == "plain-top":
+        b = 2**62 - 1 - rank * 10**7
+        return [(b - 10**7, b)], 2**32, f"plain-top: every prime in [{b - 10**7}, {b}), columns q < 2^32"
+    if name == "batched":
+        rs = batched_ranges(0)
+        mine = rs[rank::world]
+        return mine, 2**28, f"batched: {len(mine)} of 256 ranges from default_rng(0), columns q < 2^28"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
+    """The oracle (reference algorithm restated in C, all host threads) on a
+    bounded sample of rows of [lo, hi): primes per second."""
+    import oracle
+    oracle.build()
+    L = oracle.lib()
+    cores = int(L.orc_threads())
+    n = len(oracle.list_primes(lo, hi))
+    k = max(1, cores)
+    while True:
+        step = max(1, n // k)
+        sel = list(range(0, n, step))[:k]
+        t0 = time.perf_counter()
+        rows, _ = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        dt = time.perf_counter() - t0
+        if dt > budget_s / 3 or k >= n or k >= 64 * cores:
+            break
+        k *= 2
+    return {"value": len(sel) / dt, "unit": "primes/s", "cores": cores, "kind": "port",
+            "sample": f"{len(sel)} of {n} primes of [{lo}, {hi}) evenly spaced, q_cap={q_cap}, "
+                      f"{dt:.1f} s incl. the column sieve"}, rows, sel
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    ranges, q_cap, desc = workload(args.workload, 0, 1, args.width)
+    lo, hi = ranges[0]
+    import oracle
+    oracle.build()
+    cores = int(oracle.lib().orc_threads())
+    n = len(oracle.list_primes(lo, hi))
+    # a step: `k` evenly spaced rows of the workload with all columns (~5 s)
+    k = max(1, cores)
+    sel = list(range(0, n, max(1, n // k)))[:k]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = len(sel) * len(times) / tot
+    line = {
+        "metric": "primes tested/s", "value": value, "unit": "primes/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": desc, "sample_rows_per_step": len(sel), "rows_in_workload": n},
+        "cpu_baseline": {"value": value, "unit": "primes/s", "cores": cores, "kind": "port",
+                         "sample": f"{len(sel)} of {n} primes per step, evenly spaced"},
+        "e2e": {"value": value, "unit": "primes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain-small", choices=["plain-small", "plain-mid", "plain-top", "batched"])
+    ap.add_argument("--width", type=int, default=PLAIN_SMALL[1],
+                    help="plain-small range width per GPU (default 1e6; smaller only for profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    import clwilson_b200 as wl
+    eng = wl.Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+    ranges, q_cap, desc = workload(args.workload, rank, world, args.width)
+    L = max(limbs_for(b - 1) for a, b in ranges)
+    peak_mad = wl.probe("mad", local)
+    peak_cell = wl.probe("cell%d" % L, local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MiB > L2
+
+    def step():
+        eng.drop_columns()
+        if len(ranges) == 1 and q_cap == 0:
+            r = eng.search(ranges[0][0], ranges[0][1])
+            return r.stats
+        per, res, st = eng.batch(ranges, q_cap=q_cap)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    dev_ms, wall_s, stats = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.add_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t0 = time.perf_counter()
+            st = step()
+            t1 = time.perf_counter()
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms.append(e0.elapsed_time(e1))
+            wall_s.append(t1 - t0)
+            stats.append(st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    tested = sum(s.tested for s in stats)
+    tot_dev = sum(dev_ms) / 1e3
+    tot_wall = sum(wall_s)
+    sweep_s = sum(s.ms_sweep for s in stats) / 1e3
+    cells = sum(s.cells for s in stats)
+    launches = sum(s.kernel_launches for s in stats)
+    h2d = stats[-1].h2d_bytes
+    d2h = stats[-1].d2h_bytes
+    if dist:
+        t = torch.tensor([tot_dev, tot_wall, sweep_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_dev, tot_wall, sweep_max = t.tolist()
+        c = torch.tensor([tested, cells, launches], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        tested_all, cells_all, _ = c.tolist()
+    else:
+        tested_all, cells_all = tested, cells
+
+    full = q_cap == 0
+    achieved = cells * OPS_PER_CELL[L] / sweep_s / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload)
+        except Exception:
+            traffic = None
+    line = {
+        "metric": "primes tested/s" if full else "128-bit mulmods/s (capped column sweep)",
+        "value": (tested_all / tot_dev) if full else (cells_all / tot_dev),
+        "unit": "primes/s" if full else "mulmods/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_dev / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": desc, "q_cap": q_cap, "limbs": L, "test_primes_per_step": tested_all / args.steps,
+                   "column_mulmods_per_step": cells_all / args.steps,
+                   "tail_steps_per_step": sum(s.tail_steps for s in stats) / args.steps,
+                   "l2": "256 MiB buffer written between steps", "columns": "re-sieved every step",
+                   "parallelism": f"rows sharded by range, dp{world}"},
+        "mulmods_per_s": cells_all / tot_dev,
+        "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_mad / 1e12, "unit": "TOP/s",
+                     "frac": achieved * 1e12 / peak_mad, "traffic": traffic,
+                     "kernel": f"k_sweep<{L},*>", "ops_per_cell": OPS_PER_CELL[L],
+                     "cell_peak_per_s": peak_cell, "cell_frac": (cells / sweep_s) / peak_cell,
+                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
+        "e2e": {"value": (tested_all / tot_wall) if full else (cells_all / tot_wall),
+                "unit": "primes/s" if full else "mulmods/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "phase_ms_per_step": {k: sum(getattr(s, "ms_" + k) for s in stats) / args.steps
+                              for k in ("primes", "sieve", "sweep", "iterate", "finish")},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        lo, hi = ranges[0]
+        cb, _, _ = cpu_baseline(lo, hi, q_cap)
+        if not full:
+            cb["note"] = "capped sweep: value is primes/s of the capped partial products"
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

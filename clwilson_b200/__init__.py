@@ -74,7 +74,8 @@ assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
-           "wl_batch", "wl_parse_uint64")
+           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe")
+PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
 
 _lib = None
 
@@ -107,6 +108,10 @@ def load_library(path: str = LIB_PATH):
     L.wl_batch.restype = ctypes.c_int
     L.wl_parse_uint64.argtypes = [ctypes.POINTER(u64), ctypes.c_char_p, u64, u64]
     L.wl_parse_uint64.restype = ctypes.c_int
+    L.wl_drop_columns.argtypes = [vp]
+    L.wl_drop_columns.restype = None
+    L.wl_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.wl_probe.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -117,6 +122,16 @@ def parse_uint64(text: str, lo: int, hi: int) -> Tuple[int, int]:
     v = ctypes.c_uint64(0)
     rc = L.wl_parse_uint64(ctypes.byref(v), text.encode(), lo, hi)
     return rc, v.value
+
+
+def probe(which: str, device: int = 0) -> float:
+    """Integer-pipe microbenchmark (include/wilson_probe.h): operations or cells per second."""
+    L = load_library()
+    r = ctypes.c_double(0)
+    rc = L.wl_probe(device, PROBES[which], ctypes.byref(r))
+    if rc:
+        raise WilsonError(rc, "wl_probe")
+    return r.value
 
 
 def check_range(pmin: int, pmax: int) -> int:
@@ -205,6 +220,9 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+    def drop_columns(self) -> None:
+        self._L.wl_drop_columns(self._ctx)
 
     @property
     def stream(self) -> int:

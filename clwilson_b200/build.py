@@ -16,7 +16,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libwilson.so")
 CLI = os.path.join(PKG, "clwilson")
 
-CU_SOURCES = ["wl_kernels.cu", "wl_engine.cu"]
+CU_SOURCES = ["wl_kernels.cu", "wl_engine.cu", "wl_probe.cu"]
 HEADERS = ["wl_arith.cuh", "wl_internal.h"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
@@ -42,7 +42,7 @@ def _stale(target: str, deps) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS] + [os.path.join(INCLUDE, "wilson.h")]
+    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS] + [os.path.join(INCLUDE, "wilson.h"), os.path.join(INCLUDE, "wilson_probe.h")]
     if force or _stale(LIB, deps):
         objs = []
         bdir = os.path.join(PKG, "_build")

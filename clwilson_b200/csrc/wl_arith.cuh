@@ -113,6 +113,62 @@ __device__ __forceinline__ void cell(Res<4>& x, uint32_t q, const uint32_t* n, u
           "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]), "r"(ninv));
 }
 
+// The same step with 32x32->64 products (mad.wide.u32): the two product rows
+// x*q and m*n are formed as chains of 64-bit partial sums, so carries become
+// 64-bit additions on the integer ALU instead of carry-flag multiplies.
+// 2L wide multiplies + 1 low multiply.
+template <int L>
+__host__ __device__ __forceinline__ void cell_w(Res<L>& x, uint32_t q, const uint32_t* n, uint32_t ninv) {
+    uint64_t P = (uint64_t)x.w[0] * q;
+    const uint32_t t0 = (uint32_t)P;
+    uint32_t X[L];                                   // (x*q) >> 32, L limbs
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        P = (uint64_t)x.w[k] * q + (P >> 32);
+        X[k - 1] = (uint32_t)P;
+    }
+    X[L - 1] = (uint32_t)(P >> 32);
+    const uint32_t m = t0 * ninv;
+    uint64_t A = (uint64_t)m * n[0] + t0;            // low word is zero
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        A = (uint64_t)m * n[k] + X[k - 1] + (A >> 32);
+        x.w[k - 1] = (uint32_t)A;
+    }
+    x.w[L - 1] = X[L - 1] + (uint32_t)(A >> 32);
+}
+
+// As cell_w, with the first reduction product replaced by its high half:
+// lo(m*n0) = -t0 mod 2^32, so (m*n0 + t0) >> 32 = hi(m*n0) + (t0 != 0).
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+template <int L>
+__host__ __device__ __forceinline__ void cell_h(Res<L>& x, uint32_t q, const uint32_t* n, uint32_t ninv) {
+    uint64_t P = (uint64_t)x.w[0] * q;
+    const uint32_t t0 = (uint32_t)P;
+    uint32_t X[L];
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        P = (uint64_t)x.w[k] * q + (P >> 32);
+        X[k - 1] = (uint32_t)P;
+    }
+    X[L - 1] = (uint32_t)(P >> 32);
+    const uint32_t m = t0 * ninv;
+    uint64_t A = (uint64_t)(mulhi32(m, n[0]) + (t0 != 0u)) << 32;
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        A = (uint64_t)m * n[k] + X[k - 1] + (A >> 32);
+        x.w[k - 1] = (uint32_t)A;
+    }
+    x.w[L - 1] = X[L - 1] + (uint32_t)(A >> 32);
+}
+
 // x <- x - n if x >= n, as one asm block so that no compiler-generated carry
 // instruction can land inside the borrow chain; maps [0, 3n) to [0, 2n).
 __device__ __forceinline__ void cond_sub_chain(Res<3>& x, const uint32_t* n) {

@@ -82,6 +82,7 @@ int limb_width(uint64_t pmax_incl) {
 struct wl_ctx {
     int device = 0;
     int sms = 148;
+    int cell_variant = 1;   // formulation of the sweep's cell step (see wl_kernels.cu cellv)
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8] = {};
     DevBuf base;            // odd primes < 65536 (sieving primes of the column sieve)
@@ -415,7 +416,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     cudaEventRecord(c->ev[2], c->st);
     size_t ioff = 0;
     for (auto& g : groups) {
-        launch_sweep(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
+        launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
                      as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint4>(c->part), as<Deficit>(c->defs), c->st);
         if (!g.items.empty()) c->launches++;
         ioff += g.items.size();
@@ -592,6 +593,7 @@ int wl_open(int device, wl_ctx** out) {
     c->device = device;
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (const char* v = getenv("WL_CELL_VARIANT")) c->cell_variant = atoi(v);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
     for (auto& e : c->ev) cudaEventCreate(&e);
     // odd primes below 2^16: the sieving primes of the column sieve (q < 2^32)
@@ -625,6 +627,12 @@ void wl_close(wl_ctx* c) {
 }
 
 void* wl_stream(wl_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+void wl_drop_columns(wl_ctx* c) {
+    if (!c) return;
+    c->ncols = 0;
+    c->col_limit = 0;
+}
 
 int wl_search(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_cap, wl_result* results, size_t cap,
               wl_stats* stats) {

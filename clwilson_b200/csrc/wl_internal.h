@@ -80,7 +80,7 @@ void launch_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t nseg,
 void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys,
                       uint64_t* out, cudaStream_t st);
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
-void launch_sweep(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
 void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out,
                     cudaStream_t st);

@@ -269,7 +269,23 @@ __device__ __forceinline__ void fold_pow(Res<L>& A, const Res<L>& P, uint64_t d,
     A = mont_mul<L>(A, Y, n, ninv);
 }
 
-template <int L, int RPT>
+__device__ __forceinline__ uint32_t sat32(uint64_t v) { return v > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)v; }
+
+// cell step in formulation V (0: carry-flag PTX chain, 1: wide products,
+// 2: wide products with a high-half first reduction); all are exact
+template <int L, int V>
+__device__ __forceinline__ void cellv(Res<L>& x, uint32_t q, const uint32_t* n, uint32_t ninv) {
+    if (V == 0) cell(x, q, n, ninv);
+    else if (V == 1) cell_w<L>(x, q, n, ninv);
+    else cell_h<L>(x, q, n, ninv);
+}
+template <int L, int V>
+__device__ __forceinline__ void cell_wide_v(Res<L>& x, uint32_t q, const uint32_t* n, uint32_t ninv) {
+    cellv<L, V>(x, q, n, ninv);
+    cond_sub_chain(x, n);
+}
+
+template <int L, int RPT, int V>
 __global__ void __launch_bounds__(256)
 k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
         const uint32_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
@@ -302,62 +318,74 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
     u128 def = 0;
 
     if (c0 < c1) {
-        const uint64_t qf = cols[c0];
+        const uint32_t qf = cols[c0];
         uint64_t e_cur = legendre(T, qf);
-        uint64_t thr = (qf * qf > T) ? T / e_cur : qf;
-        uint64_t cells = 0;
-        uint64_t c = c0;
-        while (c < c1) {
-            if (((c & 3) == 0) && c + 4 <= c1) {
-                const uint4 g = __ldg(reinterpret_cast<const uint4*>(cols + c));
-                if ((uint64_t)g.w <= thr) {
-                    if (L == 2 || g.w < 0x80000000u) {
+        // columns q <= thr share the exponent e_cur (valid above sqrt(T));
+        // below sqrt(T) thr is the current column, so every column is checked
+        uint32_t thr = sat32(((uint64_t)qf * qf > T) ? T / e_cur : qf);
+        uint32_t cells = 0;
+        const uint32_t* cp = cols + c0;
+        const uint32_t* const ce = cols + c1;
+        while (cp < ce) {
+            if ((((uintptr_t)cp) & 31) == 0 && cp + 8 <= ce) {
+                const uint4 g0 = __ldg(reinterpret_cast<const uint4*>(cp));
+                const uint4 g1 = __ldg(reinterpret_cast<const uint4*>(cp) + 1);
+                if (g1.w <= thr) {
+                    if (L == 2 || g1.w < 0x80000000u) {
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) {
-                            cell(P[j], g.x, n[j], ninv[j]);
-                            cell(P[j], g.y, n[j], ninv[j]);
-                            cell(P[j], g.z, n[j], ninv[j]);
-                            cell(P[j], g.w, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g0.x, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g0.y, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g0.z, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g0.w, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g1.x, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g1.y, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g1.z, n[j], ninv[j]);
+                            cellv<L, V>(P[j], g1.w, n[j], ninv[j]);
                         }
                     } else {
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) {
-                            cell_wide<L>(P[j], g.x, n[j], ninv[j]);
-                            cell_wide<L>(P[j], g.y, n[j], ninv[j]);
-                            cell_wide<L>(P[j], g.z, n[j], ninv[j]);
-                            cell_wide<L>(P[j], g.w, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g0.x, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g0.y, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g0.z, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g0.w, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g1.x, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g1.y, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g1.z, n[j], ninv[j]);
+                            cell_wide_v<L, V>(P[j], g1.w, n[j], ninv[j]);
                         }
                     }
-                    c += 4;
-                    cells += 4;
+                    cp += 8;
+                    cells += 8;
                     continue;
                 }
             }
-            const uint32_t q = __ldg(cols + c);
-            if ((uint64_t)q > thr) {
+            const uint32_t q = __ldg(cp);
+            if (q > thr) {
                 const uint64_t e_new = legendre(T, q);
                 const uint64_t d = e_cur - e_new;
                 if (d) {
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
-                    def += (u128)d * (32 * cells + 32 * L);
+                    def += (u128)d * (32ull * cells + 32 * L);
                 }
                 e_cur = e_new;
-                thr = ((uint64_t)q * q > T) ? T / e_new : q;
+                thr = sat32(((uint64_t)q * q > T) ? T / e_new : q);
             }
             if (L == 2 || q < 0x80000000u) {
 #pragma unroll
-                for (int j = 0; j < RPT; ++j) cell(P[j], q, n[j], ninv[j]);
+                for (int j = 0; j < RPT; ++j) cellv<L, V>(P[j], q, n[j], ninv[j]);
             } else {
 #pragma unroll
-                for (int j = 0; j < RPT; ++j) cell_wide<L>(P[j], q, n[j], ninv[j]);
+                for (int j = 0; j < RPT; ++j) cell_wide_v<L, V>(P[j], q, n[j], ninv[j]);
             }
-            ++c;
+            ++cp;
             ++cells;
         }
 #pragma unroll
         for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], e_cur, n[j], ninv[j]);
-        def += (u128)e_cur * (32 * cells + 32 * L);
+        def += (u128)e_cur * (32ull * cells + 32 * L);
     }
 
 #pragma unroll
@@ -685,14 +713,21 @@ void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaSt
     if (!nrows) return;
     k_setup_rows<<<(nrows + 255) / 256, 256, 0, st>>>(info, nrows, mods);
 }
-void launch_sweep(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
-                  const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
-    if (!nitems) return;
-#define WL_SWEEP(LL, RR) k_sweep<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs)
+template <int V>
+static void launch_sweep_v(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                           const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+#define WL_SWEEP(LL, RR) k_sweep<LL, RR, V><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs)
     if (L == 2) { if (rpt == 2) WL_SWEEP(2, 2); else WL_SWEEP(2, 1); }
     else if (L == 3) { if (rpt == 2) WL_SWEEP(3, 2); else WL_SWEEP(3, 1); }
     else { if (rpt == 2) WL_SWEEP(4, 2); else WL_SWEEP(4, 1); }
 #undef WL_SWEEP
+}
+void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+    if (!nitems) return;
+    if (variant == 0) launch_sweep_v<0>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
+    else if (variant == 2) launch_sweep_v<2>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
+    else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
 }
 void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out, cudaStream_t st) {
     if (!nitems) return;

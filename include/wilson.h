@@ -24,6 +24,9 @@
  *                         the per-prime quotient of processResult (691-900)
  *   wl_batch              many ranges in one device pass (no counterpart: the
  *                         reference runs one range per process)
+ *   wl_drop_columns       makes the next search sieve its columns again, as the
+ *                         reference does on every run (getPrimes,
+ *                         cl_wilson.cpp:1368-1397)
  *   wl_parse_uint64       the CLI number parser parse_uint64 (putil.c:34-116)
  *   wl_check_range        setupSearch's range rules (cl_wilson.cpp:1146-1181,
  *                         main.cpp:50-56)
@@ -130,6 +133,9 @@ int wl_rows(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_cap,
 int wl_batch(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap,
              wl_range_result *out, wl_result *results, size_t cap, size_t *nresults,
              wl_stats *stats);
+
+/* Forget the resident column table; the next call sieves it again. */
+void wl_drop_columns(wl_ctx *ctx);
 
 /* parse_uint64 of the reference CLI: returns 0, -1 (cannot parse) or -2 (out of range). */
 int wl_parse_uint64(uint64_t *result, const char *str, uint64_t lo, uint64_t hi);

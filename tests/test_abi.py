@@ -11,8 +11,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "wilson.h")).read()
-    return sorted(set(re.findall(r"\b(wl_[a-z0-9_]+)\s*\(", text)))
+    import glob
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        names |= set(re.findall(r"\b(wl_[a-z0-9_]+)\s*\(", open(h).read()))
+    return sorted(names)
 
 
 def test_library_loads_and_exports_header_symbols():

@@ -31,6 +31,7 @@ ERRORS = {
     -1: "invalid argument or range", -2: "CUDA error", -3: "there are no primes to test in this range!",
     -4: "configuration not supported by this build", -5: "Wilson quotient check failed",
     -6: "representation a, c or u not found", -7: "result buffer too small", -8: "device allocation failed",
+    -9: "request exceeds the fixed scratch of the no-allocation entry point",
 }
 
 
@@ -74,7 +75,7 @@ assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
-           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe")
+           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe", "wl_column_product_noalloc")
 PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
 
 _lib = None
@@ -112,6 +113,8 @@ def load_library(path: str = LIB_PATH):
     L.wl_drop_columns.restype = None
     L.wl_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.wl_probe.restype = ctypes.c_int
+    L.wl_column_product_noalloc.argtypes = [vp, ctypes.c_uint32, u64, u64, vp, ctypes.c_uint32, vp, vp]
+    L.wl_column_product_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 

@@ -16,7 +16,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libwilson.so")
 CLI = os.path.join(PKG, "clwilson")
 
-CU_SOURCES = ["wl_kernels.cu", "wl_engine.cu", "wl_probe.cu"]
+CU_SOURCES = ["wl_kernels.cu", "wl_engine.cu", "wl_probe.cu", "wl_noalloc.cu"]
 HEADERS = ["wl_arith.cuh", "wl_internal.h"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17",

@@ -571,6 +571,7 @@ const char* wl_strerror(int code) {
         case WL_ERR_NO_REPR: return "representation a, c or u not found";
         case WL_ERR_CAPACITY: return "result buffer too small";
         case WL_ERR_NOMEM: return "device allocation failed";
+        case WL_ERR_TOO_LARGE: return "request exceeds the fixed scratch of the no-allocation entry point";
         default: return "unknown error";
     }
 }

@@ -51,6 +51,7 @@ extern "C" {
 #define WL_ERR_NO_REPR      (-6)   /* a, c or u not found (cl_wilson.cpp:554-558) */
 #define WL_ERR_CAPACITY     (-7)   /* caller buffer too small; *_needed tells the size */
 #define WL_ERR_NOMEM        (-8)   /* device allocation failed */
+#define WL_ERR_TOO_LARGE    (-9)   /* request exceeds the fixed scratch of wl_column_product_noalloc */
 
 /* reference limits (cl_wilson.h:8, cl_wilson.cpp:1162) */
 #define WL_MAXP      4611686018427387903ULL   /* (2^64-1)/4 */
@@ -136,6 +137,41 @@ int wl_batch(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap,
 
 /* Forget the resident column table; the next call sieves it again. */
 void wl_drop_columns(wl_ctx *ctx);
+
+/* Column product of one class without any device allocation.
+ *
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they run -- hosts that reserve all device memory in their own
+ * pool at start-up and forbid cudaMalloc afterwards (cudaMalloc and cudaFree
+ * synchronise the device and fail once the pool holds the memory), or paths
+ * that must not take the driver's allocation lock.
+ *
+ * For each row i, with p = primes[i]:
+ *     s0s1[2i] + p * s0s1[2i+1] = prod_{j < ncols} cols[j]^{v(cols[j], T!)}  mod p^2
+ * where v(q, T!) is the exponent of q in T! -- the same partial product that
+ * wl_rows() returns for one class with q_cap (cols = the primes q < q_cap, q <= T,
+ * ascending; T = that class's target).
+ *   primes  device array of nrows odd primes, 5 <= p < p_bound <= WL_MAXP + 1
+ *   cols    device array of ncols ascending primes, each <= T and < 2^32
+ *   s0s1    device array of 2 * nrows uint64_t (output)
+ *   stream  the cudaStream_t to run on (NULL: the legacy default stream); the
+ *           call returns once the work is queued, like a kernel launch
+ * All intermediate data lives in one fixed array of WL_NOALLOC_SCRATCH_BYTES
+ * (5 MiB) of device memory that the CUDA runtime places on every GPU that
+ * loads the library and keeps until the process exits.  Limits: nrows <=
+ * WL_NOALLOC_MAX_ROWS and (column splits x nrows) <= WL_NOALLOC_MAX_PARTIALS;
+ * larger requests return WL_ERR_TOO_LARGE.  The call uses the current CUDA
+ * device; its first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Calls share the array and each call overwrites everything it reads before
+ * reading it (nothing has to start at zero); calls that overlap on the GPU
+ * (different streams, or another host thread) race on it and must be
+ * serialised by the caller. */
+#define WL_NOALLOC_MAX_ROWS      4096u
+#define WL_NOALLOC_MAX_PARTIALS  (1u << 18)
+#define WL_NOALLOC_SCRATCH_BYTES (5u << 20)
+int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p_bound, uint64_t T,
+                              const uint32_t *cols, uint32_t ncols, uint64_t *s0s1, void *stream);
 
 /* parse_uint64 of the reference CLI: returns 0, -1 (cannot parse) or -2 (out of range). */
 int wl_parse_uint64(uint64_t *result, const char *str, uint64_t lo, uint64_t hi);

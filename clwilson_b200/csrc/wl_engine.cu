@@ -90,7 +90,7 @@ struct wl_ctx {
     DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
     uint64_t ncols = 0, col_limit = 0;
     DevBuf bitmap, segcount, offsets;
-    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, iitems, part, ipart, defs, rowout;
+    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout;
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
@@ -278,9 +278,20 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     uint64_t maxt0 = std::max(rs[0].T[0], std::max(rs[0].T[1], rs[0].T[2]));
     if (full && need > (1ull << 32)) return WL_ERR_UNSUPPORTED;
     RC(ensure_columns(c, need));
-    RC(ensure(c->keys, (hb.size() + 1) * 8));
-    RC(ensure(c->counts, (hb.size() + 1) * 8));
     keys.push_back(full ? maxt0 : std::min(maxt0, qcap - 1));
+    // dense columns: q below the point where the exponent still drops at about
+    // one prime in 16 (floor(T/q) changes when T*ln(q)/q^2 >~ 1/16); q <= sqrt(T)
+    // is always dense (Legendre terms beyond T/q)
+    const size_t nb = hb.size();
+    for (size_t i = 0; i < nb; ++i) {
+        const double T = (double)hb[i].T;
+        double q = std::sqrt(T) + 2;
+        for (int k = 0; k < 4; ++k) q = std::sqrt(16.0 * T * std::log(std::max(q, 3.0))) + 2;
+        uint64_t qd = q >= 1.8e19 ? ~0ull : (uint64_t)q;
+        keys.push_back(std::min<uint64_t>(qd, keys[i]));
+    }
+    RC(ensure(c->keys, keys.size() * 8));
+    RC(ensure(c->counts, keys.size() * 8));
     CK(cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st));
     launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->keys), (uint32_t)keys.size(),
                      as<uint64_t>(c->counts), c->st);
@@ -291,24 +302,28 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     CK(cudaGetLastError());
     c->h2d += keys.size() * 8;
     c->d2h += keys.size() * 8;
-    out.pi_maxtarget = ncol.back();
+    out.pi_maxtarget = ncol[nb];
+    const uint64_t* ndn = ncol.data() + nb + 1;   // dense column counts per bucket
 
     // ---- 4. device layout: rows, buckets, splits, items ------------------------
     std::vector<Bucket> db(hb.size());
     std::vector<RowInfo> ri(nrows);
     std::vector<uint64_t> row_src(nrows);    // global output index (range-major, ascending p)
+    // work weights: a dense column costs about 4 sparse ones
+    constexpr double DENSE_WEIGHT = 4.0;
     double W = 0;
-    for (size_t i = 0; i < hb.size(); ++i) W += (double)hb[i].primes.size() * (double)ncol[i];
+    for (size_t i = 0; i < nb; ++i)
+        W += (double)hb[i].primes.size() * ((double)(ncol[i] - ndn[i]) + DENSE_WEIGHT * (double)ndn[i]);
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
     uint32_t row = 0;
     uint64_t part_total = 0;
     uint32_t def_total = 0;
     out.cells = 0;
-    struct ItemGroup { int L, rpt; std::vector<SweepItem> items; };
+    struct ItemGroup { int L, rpt; bool dense; std::vector<SweepItem> items; };
     std::vector<ItemGroup> groups;
-    auto group_for = [&](int L, int rpt) -> std::vector<SweepItem>& {
-        for (auto& g : groups) if (g.L == L && g.rpt == rpt) return g.items;
-        groups.push_back({ L, rpt, {} });
+    auto group_for = [&](int L, int rpt, bool dense) -> std::vector<SweepItem>& {
+        for (auto& g : groups) if (g.L == L && g.rpt == rpt && g.dense == dense) return g.items;
+        groups.push_back({ L, rpt, dense, {} });
         return groups.back().items;
     };
     for (uint32_t oi = 0; oi < border.size(); ++oi) {
@@ -326,27 +341,49 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         if (b.nrows >= 512) { rpt = 2; tps = 256; }
         else if (b.nrows >= 256) { rpt = 1; tps = 256; }
         else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
-        uint64_t S = 1;
-        if (b.ncols > 0 && W > 0) {
-            S = (uint64_t)std::ceil((double)rpt * (double)b.ncols * target_threads / W);
-            const uint64_t min_split = 2048;
-            S = std::min<uint64_t>(S, std::max<uint64_t>(1, b.ncols / min_split));
-            S = std::max<uint64_t>(S, 1);
+        const uint64_t nd = ndn[i], ns = b.ncols - nd;
+        uint64_t Sd = 0, Ss = 0;
+        if (nd > 0) {
+            Sd = (uint64_t)std::ceil(DENSE_WEIGHT * (double)nd * target_threads / W);
+            // short dense splits: their cost per column varies a lot (it grows
+            // with the exponent span), so many small ones balance better
+            Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
+            Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
         }
-        b.nsplit = (uint32_t)S;
+        if (ns > 0) {
+            Ss = (uint64_t)std::ceil((double)rpt * (double)ns * target_threads / W);
+            Ss = std::max<uint64_t>(1, std::min<uint64_t>(Ss, std::max<uint64_t>(1, ns / 2048)));
+        }
+        if (Sd + Ss == 0) Ss = 1;
+        b.cdense = (uint32_t)nd;
+        b.ndense = (uint32_t)Sd;
+        b.nsplit = (uint32_t)(Sd + Ss);
+        const uint64_t S = b.nsplit;
         b.part_base = part_total;
         b.def_base = def_total;
         part_total += S * b.nrows;
         def_total += (uint32_t)S;
         out.cells += (uint64_t)b.nrows * b.ncols;
-        auto& items = group_for((int)b.L, rpt);
-        if (tps == 256) {
-            const uint32_t tile = 256 * rpt;
-            for (uint32_t r0 = 0; r0 < b.nrows; r0 += tile)
-                for (uint32_t s = 0; s < S; ++s) items.push_back({ oi, r0, s, 256u });
-        } else {
-            const uint32_t per = 256 / tps;
-            for (uint32_t s = 0; s < S; s += per) items.push_back({ oi, 0, s, (uint32_t)tps });
+        if (Ss) {
+            auto& items = group_for((int)b.L, rpt, false);
+            if (tps == 256) {
+                const uint32_t tile = 256 * rpt;
+                for (uint32_t r0 = 0; r0 < b.nrows; r0 += tile)
+                    for (uint32_t s2 = (uint32_t)Sd; s2 < S; ++s2) items.push_back({ oi, r0, s2, 256u });
+            } else {
+                const uint32_t per = 256 / tps;
+                for (uint32_t s2 = (uint32_t)Sd; s2 < S; s2 += per) items.push_back({ oi, 0, s2, (uint32_t)tps });
+            }
+        }
+        if (Sd) {
+            auto& items = group_for((int)b.L, 1, true);
+            if (tps == 256) {
+                for (uint32_t r0 = 0; r0 < b.nrows; r0 += 256)
+                    for (uint32_t s2 = 0; s2 < Sd; ++s2) items.push_back({ oi, r0, s2, 256u });
+            } else {
+                const uint32_t per = 256 / tps;
+                for (uint32_t s2 = 0; s2 < Sd; s2 += per) items.push_back({ oi, 0, s2, (uint32_t)tps });
+            }
         }
         for (uint32_t k = 0; k < b.nrows; ++k) {
             RowInfo& x = ri[row + k];
@@ -360,30 +397,26 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         }
         row += b.nrows;
     }
-    // consecutive-integer tail items (full search only)
-    std::vector<IterItem> it;
-    std::vector<std::pair<uint32_t, uint32_t>> it_groups;   // per limb width: [begin, end)
+    // consecutive-integer tail (full search only): row r has it_count chunks of
+    // K integers starting at T+1; the items themselves are derived on the device
+    uint64_t n_items = 0, K = 1;
     out.tail = 0;
     if (full) {
         uint64_t Wt = 0;
         for (uint32_t r = 0; r < nrows; ++r) Wt += ri[r].Tp - db[ri[r].bucket].T;
         out.tail = Wt;
         const double tgt_items = (double)c->sms * 2048.0 * 2.0;
-        uint64_t K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / tgt_items));
+        K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / tgt_items));
         K = std::min<uint64_t>(K, 1u << 30);
         for (uint32_t r = 0; r < nrows; ++r) {
-            const uint64_t T = db[ri[r].bucket].T;
-            const uint64_t len = ri[r].Tp - T;
-            ri[r].it_begin = (uint32_t)it.size();
-            for (uint64_t a = 0; a < len; a += K) {
-                IterItem x;
-                x.start = T + 1 + a;
-                x.row = r;
-                x.len = (uint32_t)std::min<uint64_t>(K, len - a);
-                it.push_back(x);
-            }
-            ri[r].it_count = (uint32_t)(it.size() - ri[r].it_begin);
+            const uint64_t len = ri[r].Tp - db[ri[r].bucket].T;
+            ri[r].it_begin = (uint32_t)n_items;
+            ri[r].it_count = (uint32_t)((len + K - 1) / K);
+            n_items += ri[r].it_count;
         }
+        if (n_items >= (1ull << 32)) return WL_ERR_UNSUPPORTED;
+    } else {
+        for (uint32_t r = 0; r < nrows; ++r) { ri[r].it_begin = 0; ri[r].it_count = 0; }
     }
 
     // ---- 5. upload and launch ----------------------------------------------------
@@ -393,9 +426,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     RC(ensure(c->rowinfo, (size_t)nrows * sizeof(RowInfo)));
     RC(ensure(c->rowmod, (size_t)nrows * sizeof(RowMod)));
     RC(ensure(c->items, nitems_total * sizeof(SweepItem) + 16));
-    RC(ensure(c->iitems, it.size() * sizeof(IterItem) + 16));
     RC(ensure(c->part, part_total * 16 + 16));
-    RC(ensure(c->ipart, it.size() * 16 + 16));
+    RC(ensure(c->ipart, n_items * 16 + 16));
     RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
     RC(ensure(c->rowout, (size_t)nrows * sizeof(RowOut)));
     CK(cudaMemcpyAsync(c->buckets.p, db.data(), db.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
@@ -406,18 +438,21 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     if (!all_items.empty())
         CK(cudaMemcpyAsync(c->items.p, all_items.data(), all_items.size() * sizeof(SweepItem),
                            cudaMemcpyHostToDevice, c->st));
-    if (!it.empty())
-        CK(cudaMemcpyAsync(c->iitems.p, it.data(), it.size() * sizeof(IterItem), cudaMemcpyHostToDevice, c->st));
-    c->h2d += db.size() * sizeof(Bucket) + (size_t)nrows * sizeof(RowInfo) + all_items.size() * sizeof(SweepItem) +
-              it.size() * sizeof(IterItem);
+    c->h2d += db.size() * sizeof(Bucket) + (size_t)nrows * sizeof(RowInfo) + all_items.size() * sizeof(SweepItem);
 
     launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
     c->launches++;
     cudaEventRecord(c->ev[2], c->st);
     size_t ioff = 0;
     for (auto& g : groups) {
-        launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
-                     as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint4>(c->part), as<Deficit>(c->defs), c->st);
+        if (g.dense)
+            launch_sweep_dense(g.L, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
+                               as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint4>(c->part), as<Deficit>(c->defs),
+                               c->st);
+        else
+            launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
+                         as<SweepItem>(c->items) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->cols),
+                         as<uint4>(c->part), as<Deficit>(c->defs), c->st);
         if (!g.items.empty()) c->launches++;
         ioff += g.items.size();
     }
@@ -437,15 +472,16 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         const uint32_t last = g.second.second - 1;
         const uint32_t ie = ri[last].it_begin + ri[last].it_count;
         if (ie > ib) {
-            launch_iterate(g.first, as<IterItem>(c->iitems) + ib, ie - ib, as<RowMod>(c->rowmod),
-                           as<uint4>(c->ipart) + ib, c->st);
+            launch_iterate(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                           g.second.first, g.second.second - g.second.first, ib, ie - ib, K, as<uint4>(c->ipart),
+                           c->st);
             c->launches++;
         }
     }
     cudaEventRecord(c->ev[4], c->st);
     for (auto& g : lgroups) {
         launch_finish(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
-                      as<uint4>(c->part), as<Deficit>(c->defs), as<IterItem>(c->iitems), as<uint4>(c->ipart),
+                      as<uint4>(c->part), as<Deficit>(c->defs), K, as<uint4>(c->ipart),
                       g.second.first, g.second.second - g.second.first, full ? 1 : 0, as<RowOut>(c->rowout), c->st);
         c->launches++;
     }
@@ -619,7 +655,7 @@ void wl_close(wl_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     DevBuf* bufs[] = { &c->base, &c->cols, &c->bitmap, &c->segcount, &c->offsets, &c->tp, &c->keys, &c->counts,
-                       &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->iitems, &c->part, &c->ipart,
+                       &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart,
                        &c->defs, &c->rowout };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);

@@ -33,7 +33,22 @@ struct Bucket {
     uint32_t L;          // limb width (2, 3, 4)
     uint32_t type;       // 0: p = 1 mod 3, 1: p = 5 mod 12, 2: p = 11 mod 12
     uint32_t range;      // index of the range this bucket belongs to
+    uint32_t cdense;     // columns [0, cdense) take the dense sweep (exponent changes at
+                         // nearly every column), [cdense, ncols) the prefix-fold sweep
+    uint32_t ndense;     // splits 0 .. ndense-1 cover the dense columns, the rest the others
 };
+
+// Column range [c0, c1) of split s of a bucket.
+__host__ __device__ inline void split_range(const Bucket& b, uint32_t s, uint64_t* c0, uint64_t* c1) {
+    if (s < b.ndense) {
+        *c0 = (uint64_t)b.cdense * s / b.ndense;
+        *c1 = (uint64_t)b.cdense * (s + 1) / b.ndense;
+    } else {
+        const uint64_t n = b.ncols - b.cdense, k = b.nsplit - b.ndense, j = s - b.ndense;
+        *c0 = b.cdense + n * j / k;
+        *c1 = b.cdense + n * (j + 1) / k;
+    }
+}
 
 // One CTA of the column sweep: threads [k*tps, (k+1)*tps) work on split
 // split0 + k; thread i of a group takes rows row0 + i + j*tps, j < RPT.
@@ -41,20 +56,13 @@ struct SweepItem {
     uint32_t bucket, row0, split0, tps;
 };
 
-// One thread of the consecutive-integer tail: N = start .. start+len-1.
-struct IterItem {
-    uint64_t start;
-    uint32_t row;
-    uint32_t len;
-};
-
 // Per-row state beyond the modulus.
 struct RowInfo {
     uint64_t p;
     uint64_t Tp;         // own target (p-1)/6, /4 or /2
     uint32_t bucket;
-    uint32_t it_begin;   // iterate items [it_begin, it_begin + it_count)
-    uint32_t it_count;
+    uint32_t it_begin;   // tail items [it_begin, it_begin + it_count): item k multiplies
+    uint32_t it_count;   // N = T+1+k*K .. min(T+(k+1)*K, Tp), K uniform per call
     uint32_t type;
 };
 
@@ -82,10 +90,12 @@ void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
-void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out,
-                    cudaStream_t st);
+void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
+                        const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
+                    uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st);
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods,
-                   const uint4* part, const Deficit* defs, const IterItem* iitems, const uint4* ipart,
+                   const uint4* part, const Deficit* defs, uint64_t K, const uint4* ipart,
                    uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st);
 
 }  // namespace wl

@@ -8,6 +8,8 @@
 //   k_iterate<L>                   prod of consecutive integers (iterate.cl)
 //   k_finish<L>                    combine splits + tail, class lift, quotient
 //                                  (cl_wilson.cpp:691-900, find.cl)
+#include <cstdlib>
+
 #include "wl_internal.h"
 #include "wl_arith.cuh"
 
@@ -309,8 +311,8 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
     }
 
     const uint64_t T = bk.T;
-    const uint64_t c0 = (uint64_t)bk.ncols * s / bk.nsplit;
-    const uint64_t c1 = (uint64_t)bk.ncols * (s + 1) / bk.nsplit;
+    uint64_t c0, c1;
+    split_range(bk, s, &c0, &c1);
 
     Res<L> P[RPT], A[RPT];
 #pragma unroll
@@ -408,42 +410,280 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
 }
 
 // ===========================================================================
+// Dense column sweep: the same product prod q_i^{e_i} over a split, for columns
+// where e_i = v_{q_i}(T!) changes at nearly every column (q^2 < ~32 T ln T),
+// so that prefix folding would pay an exponentiation per column.
+//
+// Each exponent is split as e = H*2^s + l with l < 2^s, s chosen per split so
+// that H changes about once per 64 columns:
+//     prod q^e = (prod q^H)^(2^s) * prod q^l.
+// The first factor is the prefix-fold product on H (cheap folds, one cell per
+// column), raised to 2^s by s squarings.  The second is a windowed product
+// over 4-bit digits of l: for window j, column q goes into bucket
+// B[digit_j(l)] (one cell), and prod_d B_d^d is formed with two running
+// products.  Windows are combined from the top (Horner).  Cost: about
+// 1 + s/4 cells per column.
+//
+// The exponents are the same for every row of the bucket, so they are
+// computed once per CTA per chunk of columns into shared memory.  Each CTA
+// holds 256/tps splits (groups of tps threads), each group staging its own
+// chunk.  Deficits (powers of two dropped by Montgomery steps) are uniform per
+// split and tracked exactly as in k_sweep.
+// ===========================================================================
+
+constexpr int DENSE_CHUNK = 1024;    // staged columns per CTA and pass
+constexpr int DW = 4;                // window width in bits
+constexpr int NBK = (1 << DW) - 1;   // buckets per window
+
+template <int L>
+__device__ __forceinline__ void bucket_cell(Res<L> (&B)[NBK], uint32_t d, uint32_t q, const uint32_t* n,
+                                            uint32_t ninv) {
+    switch (d) {
+#define WL_BC(k) case k: cell_w<L>(B[k - 1], q, n, ninv); break;
+        WL_BC(1) WL_BC(2) WL_BC(3) WL_BC(4) WL_BC(5) WL_BC(6) WL_BC(7) WL_BC(8)
+        WL_BC(9) WL_BC(10) WL_BC(11) WL_BC(12) WL_BC(13) WL_BC(14) WL_BC(15)
+#undef WL_BC
+        default: break;
+    }
+}
+
+template <int L, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
+              const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, uint4* __restrict__ part,
+              Deficit* __restrict__ defs) {
+    __shared__ uint32_t sq[DENSE_CHUNK];
+    __shared__ uint64_t sm[DENSE_CHUNK];
+    __shared__ uint32_t scnt[256][NBK + 1];     // cells per bucket, per split group
+    const SweepItem it = items[blockIdx.x];
+    const Bucket bk = buckets[it.bucket];
+    const uint32_t tps = it.tps;
+    const uint32_t G = 256 / tps;                 // splits in this CTA
+    const uint32_t g = threadIdx.x / tps, lt = threadIdx.x % tps;
+    const uint32_t KG = DENSE_CHUNK / G;          // staged columns per split and chunk
+    const uint32_t s = it.split0 + g;
+    const bool has_split = s < bk.ndense;
+    const uint32_t r = it.row0 + lt;
+    const bool live = has_split && r < bk.nrows;
+    const uint64_t T = bk.T;
+
+    uint32_t n[L];
+    uint32_t ninv;
+    {
+        const RowMod m = mods[bk.row_begin + (r < bk.nrows ? r : 0)];
+#pragma unroll
+        for (int k = 0; k < L; ++k) n[k] = m.n[k];
+        ninv = m.ninv;
+    }
+    uint64_t c0 = 0, c1 = 0;
+    if (has_split) split_range(bk, s, &c0, &c1);
+    // all groups run the same number of chunks so that barriers match
+    const uint64_t maxlen = ((uint64_t)bk.cdense + bk.ndense - 1) / bk.ndense;
+    const uint32_t nchunks = (uint32_t)((maxlen + KG - 1) / KG);
+
+    // exponent split e = H*2^sb + l: H changes about once per 64 columns
+    uint32_t sb = 0;
+    uint64_t e_first = 0;
+    if (c1 > c0) {
+        e_first = legendre(T, cols[c0]);
+        const uint64_t e_last = legendre(T, cols[c1 - 1]);
+        const uint64_t span = e_first - e_last;
+        const uint64_t per = (c1 - c0) / 64 + 1;
+        const uint64_t want = span / per;         // H steps wanted: span / 2^sb <= per
+        while (sb < 63 && (want >> sb) != 0) ++sb;
+        const uint32_t top = 64 - __clzll((long long)e_first);
+        if (sb > top) sb = top;
+    }
+    const uint64_t lmask = sb >= 64 ? ~0ull : ((1ull << sb) - 1);
+    const uint32_t nwin = (sb + DW - 1) / DW;
+    const uint32_t base = g * KG;
+
+    // ---- pass 0: prefix product on H ----
+    Res<L> P, A;
+    set_small<L>(P, 1);
+    set_small<L>(A, 1);
+    u128 defA = 0;
+    uint64_t h_cur = e_first >> sb;
+    uint32_t cells = 0;
+    for (uint32_t ch = 0; ch < nchunks; ++ch) {
+        __syncthreads();
+        const uint64_t cb = c0 + (uint64_t)ch * KG;
+        for (uint32_t k = lt; k < KG; k += tps) {
+            if (has_split && cb + k < c1) {
+                const uint32_t q = cols[cb + k];
+                sq[base + k] = q;
+                sm[base + k] = legendre(T, q) >> sb;
+            }
+        }
+        __syncthreads();
+        const uint32_t nh = (has_split && cb < c1) ? (uint32_t)(c1 - cb < KG ? c1 - cb : KG) : 0;
+        for (uint32_t k = 0; k < nh; ++k) {
+            const uint64_t h = sm[base + k];
+            if (h != h_cur) {
+                const uint64_t d = h_cur - h;
+                fold_pow<L>(A, P, d, n, ninv);
+                defA += (u128)d * (32ull * cells + 32 * L);
+                h_cur = h;
+            }
+            const uint32_t q = sq[base + k];
+            if (L == 2 || q < 0x80000000u) cell_w<L>(P, q, n, ninv);
+            else { cell_w<L>(P, q, n, ninv); cond_sub_chain(P, n); }
+            ++cells;
+        }
+    }
+    if (h_cur) {
+        fold_pow<L>(A, P, h_cur, n, ninv);
+        defA += (u128)h_cur * (32ull * cells + 32 * L);
+    }
+    for (uint32_t k = 0; k < sb; ++k) {               // A^(2^sb)
+        A = mont_mul<L>(A, A, n, ninv);
+        defA = 2 * defA + 32 * L;
+    }
+
+    // ---- windows over the low bits, top window first ----
+    Res<L> acc;
+    set_small<L>(acc, 1);
+    u128 defacc = 0;
+    for (int j = (int)nwin - 1; j >= 0; --j) {
+        Res<L> B[NBK];
+#pragma unroll
+        for (int d = 0; d < NBK; ++d) set_small<L>(B[d], 1);
+        __syncthreads();
+        for (uint32_t k = lt; k <= NBK; k += tps) scnt[g][k] = 0;
+        for (uint32_t ch = 0; ch < nchunks; ++ch) {
+            __syncthreads();
+            const uint64_t cb = c0 + (uint64_t)ch * KG;
+            for (uint32_t k = lt; k < KG; k += tps) {
+                if (has_split && cb + k < c1) {
+                    const uint32_t q = cols[cb + k];
+                    const uint32_t dg = (uint32_t)(((legendre(T, q) & lmask) >> (DW * j)) & NBK);
+                    sq[base + k] = q;
+                    sm[base + k] = dg;
+                    atomicAdd(&scnt[g][dg], 1u);
+                }
+            }
+            __syncthreads();
+            const uint32_t nh = (has_split && cb < c1) ? (uint32_t)(c1 - cb < KG ? c1 - cb : KG) : 0;
+            for (uint32_t k = 0; k < nh; ++k) {
+                const uint32_t d = (uint32_t)sm[base + k];
+                const uint32_t q = sq[base + k];
+                if (d) {
+                    if (L == 2 || q < 0x80000000u) bucket_cell<L>(B, d, q, n, ninv);
+                    else {
+                        bucket_cell<L>(B, d, q, n, ninv);
+                        switch (d) {
+#define WL_BS(k) case k: cond_sub_chain(B[k - 1], n); break;
+                            WL_BS(1) WL_BS(2) WL_BS(3) WL_BS(4) WL_BS(5) WL_BS(6) WL_BS(7) WL_BS(8)
+                            WL_BS(9) WL_BS(10) WL_BS(11) WL_BS(12) WL_BS(13) WL_BS(14) WL_BS(15)
+#undef WL_BS
+                            default: break;
+                        }
+                    }
+                }
+            }
+        }
+        // R = prod_d B_d^d by running products from the top bucket down
+        __syncthreads();
+        Res<L> S = B[NBK - 1], R = B[NBK - 1];
+        u128 defS = (u128)32 * scnt[g][NBK], defR = defS;
+#pragma unroll
+        for (int d = NBK - 2; d >= 0; --d) {
+            S = mont_mul<L>(S, B[d], n, ninv);
+            defS += (u128)32 * scnt[g][d + 1] + 32 * L;
+            R = mont_mul<L>(R, S, n, ninv);
+            defR += defS + 32 * L;
+        }
+        if (j == (int)nwin - 1) {
+            acc = R;
+            defacc = defR;
+        } else {
+            for (int k = 0; k < DW; ++k) {
+                acc = mont_mul<L>(acc, acc, n, ninv);
+                defacc = 2 * defacc + 32 * L;
+            }
+            acc = mont_mul<L>(acc, R, n, ninv);
+            defacc += defR + 32 * L;
+        }
+    }
+    Res<L> res = A;
+    u128 def = defA;
+    if (nwin) {
+        res = mont_mul<L>(A, acc, n, ninv);
+        def = defA + defacc + 32 * L;
+    }
+    if (live) {
+        uint4 o;
+        o.x = res.w[0];
+        o.y = res.w[1];
+        o.z = L > 2 ? res.w[2 < L ? 2 : 0] : 0;
+        o.w = L > 3 ? res.w[3 < L ? 3 : 0] : 0;
+        part[bk.part_base + (uint64_t)s * bk.nrows + r] = o;
+    }
+    if (has_split && it.row0 == 0 && lt == 0) {
+        Deficit dd;
+        dd.lo = (uint64_t)def;
+        dd.hi = (uint64_t)(def >> 64);
+        defs[bk.def_base + s] = dd;
+    }
+}
+
+// ===========================================================================
 // Consecutive-integer tail: prod_{N = start}^{start+len-1} N  (iterate.cl:30-43)
 // ===========================================================================
 
+// Tail item idx belongs to the row r with the largest it_begin <= idx (rows
+// with no tail share it_begin with the next row); it covers
+// N = T + 1 + k*K .. min(T + (k+1)*K, Tp) with k = idx - it_begin.
+__device__ __forceinline__ uint32_t tail_row(const RowInfo* __restrict__ info, uint32_t lo, uint32_t hi, uint32_t idx) {
+    // largest r in [lo, hi) with info[r].it_begin <= idx
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (info[m].it_begin <= idx) lo = m; else hi = m;
+    }
+    return lo;
+}
+
 template <int L>
 __global__ void __launch_bounds__(256)
-k_iterate(const IterItem* __restrict__ items, uint32_t nitems, const RowMod* __restrict__ mods, uint4* __restrict__ out) {
+k_iterate(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
+          uint32_t row_begin, uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
-    const IterItem it = items[i];
-    const RowMod m = mods[it.row];
+    const uint32_t idx = item_begin + i;
+    const uint32_t row = tail_row(info, row_begin, row_begin + nrows, idx);
+    const RowInfo ri = info[row];
+    const uint64_t T = buckets[ri.bucket].T;
+    const uint64_t k = idx - ri.it_begin;
+    const uint64_t start = T + 1 + k * K;
+    const uint64_t rest = ri.Tp - T - k * K;
+    const uint32_t len = (uint32_t)(rest < K ? rest : K);
+    const RowMod m = mods[row];
     uint32_t n[L];
 #pragma unroll
-    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    for (int q = 0; q < L; ++q) n[q] = m.n[q];
     Res<L> acc;
     set_small<L>(acc, 1);
-    const uint64_t last = it.start + it.len - 1;
+    const uint64_t last = start + len - 1;
     if (last < 0x80000000ull) {
-        uint32_t N = (uint32_t)it.start;
-        uint32_t k = 0;
-        for (; k + 4 <= it.len; k += 4, N += 4) {
-            cell(acc, N, n, m.ninv);
-            cell(acc, N + 1, n, m.ninv);
-            cell(acc, N + 2, n, m.ninv);
-            cell(acc, N + 3, n, m.ninv);
+        uint32_t N = (uint32_t)start;
+        uint32_t j = 0;
+        for (; j + 4 <= len; j += 4, N += 4) {
+            cell_w<L>(acc, N, n, m.ninv);
+            cell_w<L>(acc, N + 1, n, m.ninv);
+            cell_w<L>(acc, N + 2, n, m.ninv);
+            cell_w<L>(acc, N + 3, n, m.ninv);
         }
-        for (; k < it.len; ++k, ++N) cell(acc, N, n, m.ninv);
+        for (; j < len; ++j, ++N) cell_w<L>(acc, N, n, m.ninv);
     } else {
-        uint64_t N = it.start;
-        for (uint32_t k = 0; k < it.len; ++k, ++N) cell64<L>(acc, N, n, m.ninv);
+        uint64_t N = start;
+        for (uint32_t j = 0; j < len; ++j, ++N) cell64<L>(acc, N, n, m.ninv);
     }
     uint4 o;
     o.x = acc.w[0];
     o.y = acc.w[1];
     o.z = L > 2 ? acc.w[2 < L ? 2 : 0] : 0;
     o.w = L > 3 ? acc.w[3 < L ? 3 : 0] : 0;
-    out[i] = o;
+    out[idx] = o;
 }
 
 // ===========================================================================
@@ -548,7 +788,7 @@ __device__ __forceinline__ Res<L> mont_of_signed(int64_t v, const Res<L>& R2, co
 template <int L>
 __global__ void __launch_bounds__(128)
 k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
-         const uint4* __restrict__ part, const Deficit* __restrict__ defs, const IterItem* __restrict__ iitems,
+         const uint4* __restrict__ part, const Deficit* __restrict__ defs, uint64_t K,
          const uint4* __restrict__ ipart, uint32_t row_begin, uint32_t nrows, int full,
          RowOut* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -581,14 +821,16 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
     for (uint32_t k = 0; k < ri.it_count; ++k) {
         const uint32_t idx = ri.it_begin + k;
         const uint4 v = ipart[idx];
-        const IterItem it = iitems[idx];
+        const uint64_t start = bk.T + 1 + (uint64_t)k * K;
+        const uint64_t rest = ri.Tp - bk.T - (uint64_t)k * K;
+        const uint64_t len = rest < K ? rest : K;
         Res<L> y;
         y.w[0] = v.x; y.w[1] = v.y;
         if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
         if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
         X = mont_mul<L>(X, y, n, ninv);
-        const bool small = it.start + it.len - 1 < 0x80000000ull;
-        def += (u128)it.len * (small ? 32 : 64) + 32 * L;
+        const bool small = start + len - 1 < 0x80000000ull;
+        def += (u128)len * (small ? 32 : 64) + 32 * L;
     }
     // R mod n (Montgomery one), 2R mod n, R^2 mod n by doubling
     Res<L> one;
@@ -729,21 +971,36 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
     else if (variant == 2) launch_sweep_v<2>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
     else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
 }
-void launch_iterate(int L, const IterItem* items, uint32_t nitems, const RowMod* mods, uint4* out, cudaStream_t st) {
+void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
+                        const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+    if (!nitems) return;
+    static const int minb = getenv("WL_DENSE_MINB") ? atoi(getenv("WL_DENSE_MINB")) : 2;
+    if (minb == 1) {
+        if (L == 2) k_sweep_dense<2, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        else if (L == 3) k_sweep_dense<3, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        else k_sweep_dense<4, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+    } else {
+        if (L == 2) k_sweep_dense<2, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        else if (L == 3) k_sweep_dense<3, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        else k_sweep_dense<4, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+    }
+}
+void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
+                    uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st) {
     if (!nitems) return;
     const unsigned g = (nitems + 255) / 256;
-    if (L == 2) k_iterate<2><<<g, 256, 0, st>>>(items, nitems, mods, out);
-    else if (L == 3) k_iterate<3><<<g, 256, 0, st>>>(items, nitems, mods, out);
-    else k_iterate<4><<<g, 256, 0, st>>>(items, nitems, mods, out);
+    if (L == 2) k_iterate<2><<<g, 256, 0, st>>>(buckets, info, mods, row_begin, nrows, item_begin, nitems, K, out);
+    else if (L == 3) k_iterate<3><<<g, 256, 0, st>>>(buckets, info, mods, row_begin, nrows, item_begin, nitems, K, out);
+    else k_iterate<4><<<g, 256, 0, st>>>(buckets, info, mods, row_begin, nrows, item_begin, nitems, K, out);
 }
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
-                   const Deficit* defs, const IterItem* iitems, const uint4* ipart, uint32_t row_begin,
+                   const Deficit* defs, uint64_t K, const uint4* ipart, uint32_t row_begin,
                    uint32_t nrows, int full, RowOut* out, cudaStream_t st) {
     if (!nrows) return;
     const unsigned g = (nrows + 127) / 128;
-    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
-    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
-    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, iitems, ipart, row_begin, nrows, full, out);
+    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
+    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
+    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
 }
 
 }  // namespace wl

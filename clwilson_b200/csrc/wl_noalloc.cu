@@ -62,6 +62,8 @@ __global__ void k_noalloc_prep(const uint64_t* __restrict__ primes, uint32_t nro
         b.L = L;
         b.type = 0;
         b.range = 0;
+        b.cdense = 0;
+        b.ndense = 0;
         *bk = b;
     }
     if (i < nitems) {
@@ -164,7 +166,7 @@ extern "C" int wl_column_product_noalloc(const uint64_t* primes, uint32_t nrows,
     uint4* part = reinterpret_cast<uint4*>(base + OFF_PART);
     wl::launch_setup_rows(info, nrows, mods, st);
     wl::launch_sweep(1, L, 1, nitems, bk, items, mods, cols, part, defs, st);
-    wl::launch_finish(L, bk, info, mods, part, defs, nullptr, nullptr, 0, nrows, 0, out, st);
+    wl::launch_finish(L, bk, info, mods, part, defs, 1, nullptr, 0, nrows, 0, out, st);
     k_noalloc_out<<<(nrows + 255) / 256, 256, 0, st>>>(nrows, s0s1);
     if (cudaGetLastError() != cudaSuccess) return WL_ERR_CUDA;
     return 0;

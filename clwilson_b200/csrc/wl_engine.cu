@@ -61,6 +61,36 @@ int limb_width(uint64_t pmax_incl) {
     return 4;
 }
 
+// Cells per row that a dense column at prime q costs for class target T: one
+// for the prefix product plus one per 4-bit window of the low exponent bits,
+// s ~ log2(64 T ln(q) / q^2) (k_sweep_dense), at most the exponent's length.
+double dense_cells_at(double T, double q) {
+    const double e = T / (q - 1.0);
+    double sb = std::log2(std::max(1.0, 64.0 * T * std::log(q) / (q * q)));
+    sb = std::min(sb, std::log2(std::max(e, 1.0)) + 1.0);
+    return 1.0 + std::ceil(sb / 4.0);
+}
+
+// Cumulative dense cost over q in [2, qd] on a log grid: cum[k] for q = grid[k].
+void dense_cost_grid(double T, double qd, std::vector<double>& grid, std::vector<double>& cum, double* cols_est) {
+    const int N = 2048;
+    grid.assign(N + 1, 0.0);
+    cum.assign(N + 1, 0.0);
+    const double u0 = std::log(2.0), u1 = std::log(std::max(qd, 3.0));
+    const double du = (u1 - u0) / N;
+    double c = 0, n = 0;
+    grid[0] = 2.0;
+    for (int k = 1; k <= N; ++k) {
+        const double u = u0 + (k - 0.5) * du, q = std::exp(u);
+        const double dn = q * du / u;            // primes in the step ~ dq / ln q
+        n += dn;
+        c += dn * dense_cells_at(T, q);
+        grid[k] = std::exp(u0 + k * du);
+        cum[k] = c;
+    }
+    *cols_est = n;
+}
+
 }  // namespace
 
 #define CK(x)                                                        \
@@ -84,13 +114,15 @@ struct wl_ctx {
     int sms = 148;
     int cell_variant = 1;   // formulation of the sweep's cell step (see wl_kernels.cu cellv)
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;   // dense sweep, overlapped with the sparse sweep
     cudaEvent_t ev[8] = {};
+    cudaEvent_t fork = nullptr, join = nullptr;
     DevBuf base;            // odd primes < 65536 (sieving primes of the column sieve)
     uint32_t nbase = 0;
     DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
     uint64_t ncols = 0, col_limit = 0;
     DevBuf bitmap, segcount, offsets;
-    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout;
+    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout, dsplit;
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
@@ -279,14 +311,14 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     if (full && need > (1ull << 32)) return WL_ERR_UNSUPPORTED;
     RC(ensure_columns(c, need));
     keys.push_back(full ? maxt0 : std::min(maxt0, qcap - 1));
-    // dense columns: q below the point where the exponent still drops at about
-    // one prime in 16 (floor(T/q) changes when T*ln(q)/q^2 >~ 1/16); q <= sqrt(T)
-    // is always dense (Legendre terms beyond T/q)
+    // dense columns: q below the point where floor(T/q) drops at about every
+    // prime (T*ln(q)/q^2 >~ 1); there the prefix fold would pay a modular
+    // exponentiation per column, above it the fold is rarer than a cell
     const size_t nb = hb.size();
     for (size_t i = 0; i < nb; ++i) {
         const double T = (double)hb[i].T;
         double q = std::sqrt(T) + 2;
-        for (int k = 0; k < 4; ++k) q = std::sqrt(16.0 * T * std::log(std::max(q, 3.0))) + 2;
+        for (int k = 0; k < 4; ++k) q = std::sqrt(T * std::log(std::max(q, 3.0))) + 2;
         uint64_t qd = q >= 1.8e19 ? ~0ull : (uint64_t)q;
         keys.push_back(std::min<uint64_t>(qd, keys[i]));
     }
@@ -309,12 +341,22 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     std::vector<Bucket> db(hb.size());
     std::vector<RowInfo> ri(nrows);
     std::vector<uint64_t> row_src(nrows);    // global output index (range-major, ascending p)
-    // work weights: a dense column costs about 4 sparse ones
-    constexpr double DENSE_WEIGHT = 4.0;
+    // work weights: cells per row, dense columns by the cost model
+    std::vector<double> dcost(nb, 0.0);
+    std::vector<std::vector<double>> dgrid(nb), dcum(nb);
+    for (size_t i = 0; i < nb; ++i) {
+        if (!ndn[i]) continue;
+        double cols_est = 1;
+        const double qd = (double)std::min<uint64_t>(keys[nb + 1 + i], keys[i]);
+        dense_cost_grid((double)hb[i].T, qd, dgrid[i], dcum[i], &cols_est);
+        dcost[i] = dcum[i].back() * (double)ndn[i] / std::max(cols_est, 1.0);
+    }
     double W = 0;
     for (size_t i = 0; i < nb; ++i)
-        W += (double)hb[i].primes.size() * ((double)(ncol[i] - ndn[i]) + DENSE_WEIGHT * (double)ndn[i]);
+        W += (double)hb[i].primes.size() * ((double)(ncol[i] - ndn[i]) + dcost[i]);
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
+    std::vector<uint64_t> dkeys;                 // interior dense boundaries (values), all buckets
+    std::vector<uint32_t> dkeys_bucket_start, dkeys_n;
     uint32_t row = 0;
     uint64_t part_total = 0;
     uint32_t def_total = 0;
@@ -344,9 +386,9 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         const uint64_t nd = ndn[i], ns = b.ncols - nd;
         uint64_t Sd = 0, Ss = 0;
         if (nd > 0) {
-            Sd = (uint64_t)std::ceil(DENSE_WEIGHT * (double)nd * target_threads / W);
-            // short dense splits: their cost per column varies a lot (it grows
-            // with the exponent span), so many small ones balance better
+            // dense splits of equal estimated cost, each worth >= 20000 cells per
+            // row so that the per-split bucket combination stays small
+            Sd = (uint64_t)std::ceil(dcost[i] * target_threads / W);
             Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
             Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
         }
@@ -357,6 +399,18 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         if (Sd + Ss == 0) Ss = 1;
         b.cdense = (uint32_t)nd;
         b.ndense = (uint32_t)Sd;
+        b.dstart = (uint32_t)dkeys_bucket_start.size();
+        b.pad2 = 0;
+        dkeys_bucket_start.push_back((uint32_t)dkeys.size());
+        dkeys_n.push_back((uint32_t)Sd);
+        // interior boundaries at equal cumulative cost (values q: split k ends at q_k)
+        for (uint64_t k = 1; k < Sd; ++k) {
+            const std::vector<double>& cum = dcum[i];
+            const double target = cum.back() * (double)k / (double)Sd;
+            size_t j = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
+            if (j >= cum.size()) j = cum.size() - 1;
+            dkeys.push_back((uint64_t)dgrid[i][j]);
+        }
         b.nsplit = (uint32_t)(Sd + Ss);
         const uint64_t S = b.nsplit;
         b.part_base = part_total;
@@ -397,6 +451,40 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         }
         row += b.nrows;
     }
+    // dense split starts: [0, count(cols <= q_1), ..., cdense] per bucket (device order)
+    std::vector<uint32_t> dsplit;
+    {
+        std::vector<uint64_t> dcounts(dkeys.size());
+        if (!dkeys.empty()) {
+            RC(ensure(c->keys, dkeys.size() * 8));
+            RC(ensure(c->counts, dkeys.size() * 8));
+            CK(cudaMemcpyAsync(c->keys.p, dkeys.data(), dkeys.size() * 8, cudaMemcpyHostToDevice, c->st));
+            launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->keys), (uint32_t)dkeys.size(),
+                             as<uint64_t>(c->counts), c->st);
+            c->launches++;
+            CK(cudaMemcpyAsync(dcounts.data(), c->counts.p, dkeys.size() * 8, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            CK(cudaGetLastError());
+            c->h2d += dkeys.size() * 8;
+            c->d2h += dkeys.size() * 8;
+        }
+        for (uint32_t oi = 0; oi < db.size(); ++oi) {
+            Bucket& b = db[oi];
+            const uint32_t k0 = dkeys_bucket_start[oi], n = dkeys_n[oi];
+            b.dstart = (uint32_t)dsplit.size();
+            if (!n) continue;
+            dsplit.push_back(0);
+            uint32_t prev = 0;
+            for (uint32_t k = 1; k < n; ++k) {
+                uint32_t v = (uint32_t)std::min<uint64_t>(dcounts[k0 + k - 1], b.cdense);
+                v = std::max(v, prev);
+                dsplit.push_back(v);
+                prev = v;
+            }
+            dsplit.push_back(b.cdense);
+        }
+    }
+
     // consecutive-integer tail (full search only): row r has it_count chunks of
     // K integers starting at T+1; the items themselves are derived on the device
     uint64_t n_items = 0, K = 1;
@@ -430,6 +518,9 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     RC(ensure(c->ipart, n_items * 16 + 16));
     RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
     RC(ensure(c->rowout, (size_t)nrows * sizeof(RowOut)));
+    RC(ensure(c->dsplit, dsplit.size() * 4 + 16));
+    if (!dsplit.empty())
+        CK(cudaMemcpyAsync(c->dsplit.p, dsplit.data(), dsplit.size() * 4, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->buckets.p, db.data(), db.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->rowinfo.p, ri.data(), (size_t)nrows * sizeof(RowInfo), cudaMemcpyHostToDevice, c->st));
     std::vector<SweepItem> all_items;
@@ -444,17 +535,27 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     c->launches++;
     cudaEventRecord(c->ev[2], c->st);
     size_t ioff = 0;
+    bool forked = false;
     for (auto& g : groups) {
+        if (g.dense && !g.items.empty() && !forked) {
+            CK(cudaEventRecord(c->fork, c->st));
+            CK(cudaStreamWaitEvent(c->st2, c->fork, 0));
+            forked = true;
+        }
         if (g.dense)
             launch_sweep_dense(g.L, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
-                               as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint4>(c->part), as<Deficit>(c->defs),
-                               c->st);
+                               as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint32_t>(c->dsplit),
+                               as<uint4>(c->part), as<Deficit>(c->defs), c->st2);
         else
             launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
                          as<SweepItem>(c->items) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->cols),
                          as<uint4>(c->part), as<Deficit>(c->defs), c->st);
         if (!g.items.empty()) c->launches++;
         ioff += g.items.size();
+    }
+    if (forked) {
+        CK(cudaEventRecord(c->join, c->st2));
+        CK(cudaStreamWaitEvent(c->st, c->join, 0));
     }
     cudaEventRecord(c->ev[3], c->st);
     // rows are ordered by limb width: one tail and one finish launch per width
@@ -631,8 +732,14 @@ int wl_open(int device, wl_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* v = getenv("WL_CELL_VARIANT")) c->cell_variant = atoi(v);
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return WL_ERR_CUDA;
+    }
     for (auto& e : c->ev) cudaEventCreate(&e);
+    cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
     // odd primes below 2^16: the sieving primes of the column sieve (q < 2^32)
     std::vector<uint8_t> comp(65536, 0);
     std::vector<uint32_t> base;
@@ -655,10 +762,13 @@ void wl_close(wl_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     DevBuf* bufs[] = { &c->base, &c->cols, &c->bitmap, &c->segcount, &c->offsets, &c->tp, &c->keys, &c->counts,
-                       &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart,
+                       &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
                        &c->defs, &c->rowout };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
+    if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }

@@ -36,13 +36,22 @@ struct Bucket {
     uint32_t cdense;     // columns [0, cdense) take the dense sweep (exponent changes at
                          // nearly every column), [cdense, ncols) the prefix-fold sweep
     uint32_t ndense;     // splits 0 .. ndense-1 cover the dense columns, the rest the others
+    uint32_t dstart;     // dense split s covers columns [dsplit[dstart+s], dsplit[dstart+s+1])
+    uint32_t pad2;
 };
 
-// Column range [c0, c1) of split s of a bucket.
-__host__ __device__ inline void split_range(const Bucket& b, uint32_t s, uint64_t* c0, uint64_t* c1) {
+// Column range [c0, c1) of split s of a bucket.  Dense splits have explicit
+// boundaries (dsplit, balanced by estimated cost); the others are equal.
+__host__ __device__ inline void split_range(const Bucket& b, uint32_t s, uint64_t* c0, uint64_t* c1,
+                                            const uint32_t* dsplit = nullptr) {
     if (s < b.ndense) {
-        *c0 = (uint64_t)b.cdense * s / b.ndense;
-        *c1 = (uint64_t)b.cdense * (s + 1) / b.ndense;
+        if (dsplit) {
+            *c0 = dsplit[b.dstart + s];
+            *c1 = dsplit[b.dstart + s + 1];
+        } else {
+            *c0 = (uint64_t)b.cdense * s / b.ndense;
+            *c1 = (uint64_t)b.cdense * (s + 1) / b.ndense;
+        }
     } else {
         const uint64_t n = b.ncols - b.cdense, k = b.nsplit - b.ndense, j = s - b.ndense;
         *c0 = b.cdense + n * j / k;
@@ -91,7 +100,7 @@ void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaSt
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
 void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
-                        const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+                        const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st);
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
                     uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st);
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods,

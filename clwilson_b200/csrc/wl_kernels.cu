@@ -450,8 +450,8 @@ __device__ __forceinline__ void bucket_cell(Res<L> (&B)[NBK], uint32_t d, uint32
 template <int L, int MINB>
 __global__ void __launch_bounds__(256, MINB)
 k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
-              const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, uint4* __restrict__ part,
-              Deficit* __restrict__ defs) {
+              const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, const uint32_t* __restrict__ dsplit,
+              uint4* __restrict__ part, Deficit* __restrict__ defs) {
     __shared__ uint32_t sq[DENSE_CHUNK];
     __shared__ uint64_t sm[DENSE_CHUNK];
     __shared__ uint32_t scnt[256][NBK + 1];     // cells per bucket, per split group
@@ -476,9 +476,15 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
         ninv = m.ninv;
     }
     uint64_t c0 = 0, c1 = 0;
-    if (has_split) split_range(bk, s, &c0, &c1);
-    // all groups run the same number of chunks so that barriers match
-    const uint64_t maxlen = ((uint64_t)bk.cdense + bk.ndense - 1) / bk.ndense;
+    if (has_split) split_range(bk, s, &c0, &c1, dsplit);
+    // all groups of the CTA run the same number of chunks so that barriers match
+    uint64_t maxlen = 0;
+    for (uint32_t k = 0; k < G; ++k) {
+        if (it.split0 + k >= bk.ndense) break;
+        uint64_t a0, a1;
+        split_range(bk, it.split0 + k, &a0, &a1, dsplit);
+        if (a1 - a0 > maxlen) maxlen = a1 - a0;
+    }
     const uint32_t nchunks = (uint32_t)((maxlen + KG - 1) / KG);
 
     // exponent split e = H*2^sb + l: H changes about once per 64 columns
@@ -972,17 +978,17 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
     else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
 }
 void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
-                        const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+                        const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st) {
     if (!nitems) return;
     static const int minb = getenv("WL_DENSE_MINB") ? atoi(getenv("WL_DENSE_MINB")) : 2;
     if (minb == 1) {
-        if (L == 2) k_sweep_dense<2, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
-        else if (L == 3) k_sweep_dense<3, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
-        else k_sweep_dense<4, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        if (L == 2) k_sweep_dense<2, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+        else if (L == 3) k_sweep_dense<3, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+        else k_sweep_dense<4, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
     } else {
-        if (L == 2) k_sweep_dense<2, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
-        else if (L == 3) k_sweep_dense<3, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
-        else k_sweep_dense<4, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs);
+        if (L == 2) k_sweep_dense<2, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+        else if (L == 3) k_sweep_dense<3, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+        else k_sweep_dense<4, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
     }
 }
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,

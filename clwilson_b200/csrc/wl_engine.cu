@@ -123,6 +123,9 @@ struct wl_ctx {
     uint64_t ncols = 0, col_limit = 0;
     DevBuf bitmap, segcount, offsets;
     DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout, dsplit;
+    // columns above 2^32
+    cudaStream_t st3 = nullptr;
+    DevBuf bbitmap, bsegcount, boffsets, boffs, wcols, wbuckets, witems, wpart, wdefs, bacc, bdef, wkeys, wcounts;
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
@@ -192,6 +195,180 @@ struct RunOut {
     std::vector<uint64_t> range_targets;  // 3 per range
     uint64_t pi_maxtarget = 0, cells = 0, tail = 0;
 };
+
+// ---------------------------------------------------------------------------
+// columns above 2^32: windows of the number line are sieved on the device,
+// swept (k_sweep64) and merged into a per-row accumulator (k_merge) that
+// k_finish folds in.  Runs on its own stream; the main stream waits for it.
+// ---------------------------------------------------------------------------
+
+static uint64_t isqrt_u64(uint64_t n) {
+    uint64_t r = (uint64_t)std::sqrt((long double)n);
+    while (r * r > n) --r;
+    while ((r + 1) * (r + 1) <= n) ++r;
+    return r;
+}
+
+static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::vector<RowInfo>& ri, uint32_t nrows,
+                           const std::vector<uint64_t>& keys_host_order, uint64_t big_need, uint64_t maxt0, bool full,
+                           uint64_t qcap, uint64_t* pi_big) {
+    (void)keys_host_order;
+    cudaStream_t s3 = c->st3;
+    const uint64_t LO = 1ull << 32;
+    const uint64_t WIN = 1ull << 33;
+    const uint32_t SPC = 8;
+    // per-bucket upper key (device order)
+    std::vector<uint64_t> bkey(db.size());
+    for (size_t b = 0; b < db.size(); ++b) {
+        uint64_t key = db[b].T;
+        if (!full && qcap - 1 < key) key = qcap - 1;
+        bkey[b] = key;
+    }
+    // sieving primes: odd primes 67 .. isqrt(big_need - 1) from the column cache
+    // (cols[0] = 2, cols[1..17] = 3..61, cols[18] = 67)
+    const uint64_t root = isqrt_u64(big_need - 1);
+    uint64_t nroot = 0;
+    {
+        RC(ensure(c->wkeys, 16));
+        RC(ensure(c->wcounts, 16));
+        CK(cudaMemcpyAsync(c->wkeys.p, &root, 8, cudaMemcpyHostToDevice, s3));
+        launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->wkeys), 1, as<uint64_t>(c->wcounts), s3);
+        c->launches++;
+        CK(cudaMemcpyAsync(&nroot, c->wcounts.p, 8, cudaMemcpyDeviceToHost, s3));
+        CK(cudaStreamSynchronize(s3));
+    }
+    const uint32_t nbase = nroot > 18 ? (uint32_t)(nroot - 18) : 0;
+    const uint32_t* base = as<uint32_t>(c->cols) + 18;
+
+    // running per-row accumulators (raw 1) and per-bucket deficits (0)
+    RC(ensure(c->bacc, (size_t)nrows * 16 + 16));
+    RC(ensure(c->bdef, db.size() * sizeof(Deficit) + 16));
+    {
+        std::vector<uint4> ones(nrows, make_uint4(1, 0, 0, 0));
+        CK(cudaMemcpyAsync(c->bacc.p, ones.data(), (size_t)nrows * 16, cudaMemcpyHostToDevice, s3));
+        CK(cudaMemsetAsync(c->bdef.p, 0, db.size() * sizeof(Deficit), s3));
+        CK(cudaStreamSynchronize(s3));   // `ones` goes out of scope
+    }
+    // row groups by limb width (rows are ordered by width)
+    std::vector<std::pair<int, std::pair<uint32_t, uint32_t>>> lgroups;
+    for (uint32_t rb = 0; rb < nrows;) {
+        const int L = (int)db[ri[rb].bucket].L;
+        uint32_t re = rb;
+        while (re < nrows && (int)db[ri[re].bucket].L == L) ++re;
+        lgroups.push_back({ L, { rb, re } });
+        rb = re;
+    }
+    const double target_threads = (double)c->sms * 2048.0 * 4.0;
+    *pi_big = 0;
+    for (uint64_t w0 = LO; w0 < big_need; w0 += WIN) {
+        const uint64_t w1 = std::min(w0 + WIN, big_need);
+        const uint32_t nseg = (uint32_t)((w1 - w0 + BIG_SPAN - 1) / BIG_SPAN);
+        const uint32_t ncta = (nseg + SPC - 1) / SPC;
+        RC(ensure(c->bbitmap, (size_t)nseg * BIG_WORDS * 4));
+        RC(ensure(c->bsegcount, (size_t)nseg * 4));
+        RC(ensure(c->boffsets, (size_t)(nseg + 1) * 8));
+        RC(ensure(c->boffs, (size_t)ncta * std::max<uint32_t>(nbase, 1) * 4));
+        launch_sieve_big(w0, w1, nseg, SPC, base, nbase, as<uint32_t>(c->boffs), as<uint32_t>(c->bbitmap),
+                         as<uint32_t>(c->bsegcount), s3);
+        c->launches++;
+        std::vector<uint32_t> segcnt(nseg);
+        CK(cudaMemcpyAsync(segcnt.data(), c->bsegcount.p, (size_t)nseg * 4, cudaMemcpyDeviceToHost, s3));
+        CK(cudaStreamSynchronize(s3));
+        CK(cudaGetLastError());
+        std::vector<uint64_t> offs(nseg + 1);
+        uint64_t tot = 0;
+        for (uint32_t k = 0; k < nseg; ++k) { offs[k] = tot; tot += segcnt[k]; }
+        offs[nseg] = tot;
+        if (tot == 0) continue;
+        RC(ensure(c->wcols, tot * 8 + 64));
+        CK(cudaMemcpyAsync(c->boffsets.p, offs.data(), (size_t)(nseg + 1) * 8, cudaMemcpyHostToDevice, s3));
+        launch_compact_big(nseg, w0, as<uint32_t>(c->bbitmap), as<uint64_t>(c->boffsets), as<uint64_t>(c->wcols), s3);
+        c->launches++;
+        // columns of the window per bucket (<= its key), and <= maxt0 for pi(maxtarget)
+        std::vector<uint64_t> wk(db.size() + 1);
+        for (size_t b = 0; b < db.size(); ++b) wk[b] = bkey[b] >= w0 ? std::min(bkey[b], w1 - 1) : 0;
+        wk[db.size()] = maxt0;
+        RC(ensure(c->wkeys, wk.size() * 8));
+        RC(ensure(c->wcounts, wk.size() * 8));
+        CK(cudaMemcpyAsync(c->wkeys.p, wk.data(), wk.size() * 8, cudaMemcpyHostToDevice, s3));
+        launch_count_leq64(as<uint64_t>(c->wcols), tot, as<uint64_t>(c->wkeys), (uint32_t)wk.size(),
+                           as<uint64_t>(c->wcounts), s3);
+        c->launches++;
+        std::vector<uint64_t> wn(wk.size());
+        CK(cudaMemcpyAsync(wn.data(), c->wcounts.p, wk.size() * 8, cudaMemcpyDeviceToHost, s3));
+        CK(cudaStreamSynchronize(s3));
+        CK(cudaGetLastError());
+        *pi_big += wn[db.size()];
+        // window buckets and sweep items
+        std::vector<Bucket> wb(db);
+        double W = 0;
+        for (size_t b = 0; b < db.size(); ++b) {
+            if (bkey[b] < w0) wn[b] = 0;
+            W += (double)db[b].nrows * (double)wn[b];
+        }
+        if (W == 0) continue;
+        struct Grp { int L, rpt; std::vector<SweepItem> items; };
+        std::vector<Grp> groups;
+        uint64_t part_total = 0;
+        uint32_t def_total = 0;
+        for (size_t b = 0; b < db.size(); ++b) {
+            Bucket& x = wb[b];
+            x.ncols = (uint32_t)wn[b];
+            x.cdense = 0;
+            x.ndense = 0;
+            x.part_base = part_total;
+            x.def_base = def_total;
+            if (!wn[b]) { x.nsplit = 0; continue; }
+            int rpt, tps;
+            if (x.nrows >= 512) { rpt = 2; tps = 256; }
+            else if (x.nrows >= 256) { rpt = 1; tps = 256; }
+            else { rpt = 1; tps = 1; while (tps < (int)x.nrows) tps <<= 1; }
+            uint64_t S = (uint64_t)std::ceil((double)rpt * (double)wn[b] * target_threads / W);
+            S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, wn[b] / 2048)));
+            x.nsplit = (uint32_t)S;
+            part_total += S * x.nrows;
+            def_total += (uint32_t)S;
+            Grp* g = nullptr;
+            for (auto& gg : groups) if (gg.L == (int)x.L && gg.rpt == rpt) g = &gg;
+            if (!g) { groups.push_back({ (int)x.L, rpt, {} }); g = &groups.back(); }
+            if (tps == 256) {
+                for (uint32_t r0 = 0; r0 < x.nrows; r0 += 256 * rpt)
+                    for (uint32_t s2 = 0; s2 < S; ++s2) g->items.push_back({ (uint32_t)b, r0, s2, 256u });
+            } else {
+                const uint32_t per = 256 / tps;
+                for (uint32_t s2 = 0; s2 < S; s2 += per) g->items.push_back({ (uint32_t)b, 0, s2, (uint32_t)tps });
+            }
+        }
+        std::vector<SweepItem> all;
+        for (auto& g : groups) all.insert(all.end(), g.items.begin(), g.items.end());
+        RC(ensure(c->wbuckets, wb.size() * sizeof(Bucket)));
+        RC(ensure(c->witems, all.size() * sizeof(SweepItem) + 16));
+        RC(ensure(c->wpart, part_total * 16 + 16));
+        RC(ensure(c->wdefs, (size_t)def_total * sizeof(Deficit) + 16));
+        CK(cudaMemcpyAsync(c->wbuckets.p, wb.data(), wb.size() * sizeof(Bucket), cudaMemcpyHostToDevice, s3));
+        CK(cudaMemcpyAsync(c->witems.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, s3));
+        size_t ioff = 0;
+        for (auto& g : groups) {
+            launch_sweep64(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->wbuckets),
+                           as<SweepItem>(c->witems) + ioff, as<RowMod>(c->rowmod), as<uint64_t>(c->wcols),
+                           as<uint4>(c->wpart), as<Deficit>(c->wdefs), s3);
+            c->launches++;
+            ioff += g.items.size();
+        }
+        for (auto& g : lgroups) {
+            launch_merge(g.first, as<Bucket>(c->wbuckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                         as<uint4>(c->wpart), as<Deficit>(c->wdefs), g.second.first, g.second.second - g.second.first,
+                         as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
+            c->launches++;
+        }
+        // host vectors above are consumed by queued copies: wait before reuse
+        CK(cudaStreamSynchronize(s3));
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->join, s3));
+    CK(cudaStreamWaitEvent(c->st, c->join, 0));
+    return 0;
+}
 
 static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qcap, RunOut& out, wl_stats* st) {
     const bool full = (qcap == 0);
@@ -308,8 +485,11 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     }
     // the largest class target of the first range (for pi(maxtarget))
     uint64_t maxt0 = std::max(rs[0].T[0], std::max(rs[0].T[1], rs[0].T[2]));
-    if (full && need > (1ull << 32)) return WL_ERR_UNSUPPORTED;
-    RC(ensure_columns(c, need));
+    // columns above 2^32 come from the windowed sieve (run_big_columns); the
+    // cache holds every prime below min(need, 2^32), which includes the
+    // sieving primes of the windows (< 2^31)
+    const uint64_t big_need = need > (1ull << 32) ? need : 0;
+    RC(ensure_columns(c, std::min<uint64_t>(need, 1ull << 32)));
     keys.push_back(full ? maxt0 : std::min(maxt0, qcap - 1));
     // dense columns: q below the point where floor(T/q) drops at about every
     // prime (T*ln(q)/q^2 >~ 1); there the prefix fold would pay a modular
@@ -557,6 +737,13 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         CK(cudaEventRecord(c->join, c->st2));
         CK(cudaStreamWaitEvent(c->st, c->join, 0));
     }
+    bool big = false;
+    if (big_need) {
+        uint64_t pi_big = 0;
+        RC(run_big_columns(c, db, ri, nrows, keys, big_need, maxt0, full, qcap, &pi_big));
+        out.pi_maxtarget += pi_big;
+        big = true;
+    }
     cudaEventRecord(c->ev[3], c->st);
     // rows are ordered by limb width: one tail and one finish launch per width
     uint32_t rb = 0;
@@ -583,7 +770,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     for (auto& g : lgroups) {
         launch_finish(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
                       as<uint4>(c->part), as<Deficit>(c->defs), K, as<uint4>(c->ipart),
-                      g.second.first, g.second.second - g.second.first, full ? 1 : 0, as<RowOut>(c->rowout), c->st);
+                      g.second.first, g.second.second - g.second.first, full ? 1 : 0, as<RowOut>(c->rowout), c->st,
+                      big ? as<uint4>(c->bacc) : nullptr, big ? as<Deficit>(c->bdef) : nullptr);
         c->launches++;
     }
     std::vector<RowOut> ro(nrows);
@@ -733,7 +921,8 @@ int wl_open(int device, wl_ctx** out) {
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* v = getenv("WL_CELL_VARIANT")) c->cell_variant = atoi(v);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return WL_ERR_CUDA;
     }
@@ -763,12 +952,15 @@ void wl_close(wl_ctx* c) {
     cudaSetDevice(c->device);
     DevBuf* bufs[] = { &c->base, &c->cols, &c->bitmap, &c->segcount, &c->offsets, &c->tp, &c->keys, &c->counts,
                        &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
+                       &c->bbitmap, &c->bsegcount, &c->boffsets, &c->boffs, &c->wcols, &c->wbuckets, &c->witems,
+                       &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts,
                        &c->defs, &c->rowout };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->fork) cudaEventDestroy(c->fork);
     if (c->join) cudaEventDestroy(c->join);
     if (c->st2) cudaStreamDestroy(c->st2);
+    if (c->st3) cudaStreamDestroy(c->st3);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }

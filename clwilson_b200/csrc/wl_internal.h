@@ -85,6 +85,13 @@ struct RowOut {
 
 struct Deficit { uint64_t lo, hi; };
 
+// Sieve geometry above 2^32: 2^21 integers per segment (odd ones: 2^20 bits,
+// a 128 KB shared-memory bitmap), several consecutive segments per CTA.
+constexpr uint32_t BIG_SPAN = 1u << 21;
+constexpr uint32_t BIG_BITS = BIG_SPAN / 2;
+constexpr uint32_t BIG_WORDS = BIG_BITS / 32;
+constexpr uint32_t BIG_PRESIEVE = 17;   // odd primes 3..61 are removed by mask tables
+
 // Launch wrappers (wl_kernels.cu).  All are asynchronous on `st`.
 void launch_sieve_segments(uint32_t seg0, uint32_t nseg, uint64_t limit, const uint32_t* base,
                            uint32_t nbase, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
@@ -101,10 +108,21 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
 void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
                         const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t segs_per_cta, const uint32_t* base,
+                      uint32_t nbase, uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
+void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,
+                        cudaStream_t st);
+void launch_count_leq64(const uint64_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys, uint64_t* out,
+                        cudaStream_t st);
+void launch_sweep64(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
+                    const uint64_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                  const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
                     uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st);
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods,
                    const uint4* part, const Deficit* defs, uint64_t K, const uint4* ipart,
-                   uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st);
+                   uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st,
+                   const uint4* bacc = nullptr, const Deficit* bdef = nullptr);
 
 }  // namespace wl

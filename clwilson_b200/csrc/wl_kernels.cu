@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(128)
 k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
          const uint4* __restrict__ part, const Deficit* __restrict__ defs, uint64_t K,
          const uint4* __restrict__ ipart, uint32_t row_begin, uint32_t nrows, int full,
-         RowOut* __restrict__ out) {
+         RowOut* __restrict__ out, const uint4* __restrict__ bacc, const Deficit* __restrict__ bdef) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrows) return;
     const uint32_t row = row_begin + i;
@@ -837,6 +837,17 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
         X = mont_mul<L>(X, y, n, ninv);
         const bool small = start + len - 1 < 0x80000000ull;
         def += (u128)len * (small ? 32 : 64) + 32 * L;
+    }
+    // columns above 2^32, merged window by window
+    if (bacc) {
+        const uint4 v = bacc[row];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, ninv);
+        const Deficit d = bdef[ri.bucket];
+        def += (((u128)d.hi << 64) | d.lo) + 32 * L;
     }
     // R mod n (Montgomery one), 2R mod n, R^2 mod n by doubling
     Res<L> one;
@@ -930,6 +941,282 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
 }
 
 // ===========================================================================
+// Columns above 2^32.  A window [lo, hi) is sieved by CTAs that each own
+// `spc` consecutive segments of BIG_SPAN integers.  Odd primes 3..61 are
+// removed by OR-ing precomputed 32-bit masks (one table per prime, indexed by
+// the residue of the word's first number); every larger sieving prime keeps
+// its next bit offset in global memory between the CTA's segments, so its
+// starting point is divided out only once per CTA.
+// ===========================================================================
+
+constexpr uint32_t BIG_THREADS = 1024;
+__constant__ uint32_t c_pre[BIG_PRESIEVE] = { 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61 };
+__constant__ uint32_t c_preoff[BIG_PRESIEVE] = { 0, 3, 8, 15, 26, 39, 56, 75, 98, 127, 158, 195, 236, 279, 326, 379, 438 };
+constexpr uint32_t PRE_TABLE = 499;          // 3 + 5 + ... + 61
+constexpr uint32_t OFF_NONE = 0xFFFFFFFFu;   // prime does not reach this CTA's range
+
+__global__ void __launch_bounds__(BIG_THREADS)
+k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_t* __restrict__ base, uint32_t nbase,
+            uint32_t* __restrict__ offs, uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
+    extern __shared__ uint32_t smem[];
+    uint32_t* bm = smem;                  // BIG_WORDS words
+    uint32_t* tab = smem + BIG_WORDS;     // PRE_TABLE masks
+    __shared__ uint32_t wsum[BIG_THREADS / 32];
+    for (uint32_t i = threadIdx.x; i < PRE_TABLE; i += blockDim.x) {
+        uint32_t j = 0;
+        while (j + 1 < BIG_PRESIEVE && c_preoff[j + 1] <= i) ++j;
+        const uint32_t p = c_pre[j], r = i - c_preoff[j];
+        uint32_t m = 0;
+        for (uint32_t b = 0; b < 32; ++b)
+            if ((r + 2 * b) % p == 0) m |= 1u << b;    // number = (r mod p) + 2b
+        tab[i] = m;
+    }
+    const uint32_t seg0 = blockIdx.x * spc;
+    const uint64_t cta_lo = lo + (uint64_t)seg0 * BIG_SPAN;
+    const uint64_t range_bits = (uint64_t)spc * BIG_BITS;
+    uint32_t* off = offs + (uint64_t)blockIdx.x * nbase;
+    for (uint32_t k = threadIdx.x; k < nbase; k += blockDim.x) {
+        const uint64_t p = base[k];
+        uint64_t m = (cta_lo + p - 1) / p * p;
+        if (m < p * p) m = p * p;
+        if (!(m & 1)) m += p;
+        const uint64_t o = (m - cta_lo - 1) / 2;       // number = cta_lo + 2o + 1
+        off[k] = o < range_bits ? (uint32_t)o : OFF_NONE;
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < spc; ++j) {
+        const uint32_t seg = seg0 + j;
+        if (seg >= nseg) break;                          // uniform across the CTA
+        const uint64_t slo = cta_lo + (uint64_t)j * BIG_SPAN;
+        for (uint32_t w = threadIdx.x; w < BIG_WORDS; w += blockDim.x) {
+            const uint64_t n0 = slo + 64ull * w + 1;
+            uint32_t word = 0;
+#pragma unroll
+            for (uint32_t q = 0; q < BIG_PRESIEVE; ++q) word |= tab[c_preoff[q] + (uint32_t)(n0 % c_pre[q])];
+            bm[w] = word;
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < nbase; k += blockDim.x) {
+            uint32_t o = off[k];
+            if (o == OFF_NONE) continue;
+            const uint32_t p = base[k];
+            for (; o < BIG_BITS; o += p) atomicOr(&bm[o >> 5], 1u << (o & 31));
+            off[k] = o - BIG_BITS;
+        }
+        __syncthreads();
+        uint32_t cnt = 0;
+        for (uint32_t w = threadIdx.x; w < BIG_WORDS; w += blockDim.x) {
+            uint32_t pb = ~bm[w];
+            const uint64_t first = slo + 64ull * w + 1;
+            if (first + 62 >= hi) {
+                uint32_t keep = 0;
+                for (uint32_t b = 0; b < 32; ++b)
+                    if (first + 2ull * b < hi) keep |= 1u << b;
+                pb &= keep;
+            }
+            bitmap[(uint64_t)seg * BIG_WORDS + w] = pb;
+            cnt += __popc(pb);
+        }
+        for (int o2 = 16; o2 > 0; o2 >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o2);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (uint32_t i = 0; i < blockDim.x / 32; ++i) t += wsum[i];
+            seg_count[seg] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// ordered u64 write-out of a big window's bitmap (segment s: odd numbers lo0 + s*BIG_SPAN + 2i + 1)
+__global__ void __launch_bounds__(1024)
+k_compact_big(uint64_t lo0, const uint32_t* __restrict__ bitmap, const uint64_t* __restrict__ offsets,
+              uint64_t* __restrict__ out) {
+    __shared__ uint32_t wsum[32];
+    constexpr uint32_t WPT = BIG_WORDS / 1024;
+    const uint32_t seg = blockIdx.x;
+    const uint32_t* bm = bitmap + (uint64_t)seg * BIG_WORDS + threadIdx.x * WPT;
+    uint32_t cnt = 0;
+    for (uint32_t i = 0; i < WPT; ++i) cnt += __popc(bm[i]);
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (uint32_t i = 0; i < wid; ++i) wbase += wsum[i];
+    uint64_t pos = offsets[seg] + wbase + incl - cnt;
+    const uint64_t lo = lo0 + (uint64_t)seg * BIG_SPAN;
+    for (uint32_t i = 0; i < WPT; ++i) {
+        uint32_t w = bm[i];
+        const uint64_t base_n = lo + (uint64_t)(threadIdx.x * WPT + i) * 64 + 1;
+        while (w) {
+            const int b = __ffs(w) - 1;
+            w &= w - 1;
+            out[pos++] = base_n + 2ull * b;
+        }
+    }
+}
+
+__global__ void k_count_leq64(const uint64_t* __restrict__ cols, uint64_t ncols, const uint64_t* __restrict__ keys,
+                              uint32_t nkeys, uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nkeys) return;
+    const uint64_t key = keys[i];
+    uint64_t a = 0, b = ncols;
+    while (a < b) {
+        const uint64_t m = (a + b) >> 1;
+        if (cols[m] <= key) a = m + 1; else b = m;
+    }
+    out[i] = a;
+}
+
+// Sweep over 64-bit columns q > 2^32 > sqrt(T): exponent floor(T/q), prefix
+// folding as in k_sweep, each cell a two-round 64-bit Montgomery step.
+template <int L, int RPT>
+__global__ void __launch_bounds__(256)
+k_sweep64(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
+          const uint64_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
+    const SweepItem it = items[blockIdx.x];
+    const Bucket bk = buckets[it.bucket];
+    const uint32_t s = it.split0 + threadIdx.x / it.tps;
+    if (s >= bk.nsplit) return;
+    const uint32_t rl = it.row0 + threadIdx.x % it.tps;
+    uint32_t n[RPT][L];
+    uint32_t ninv[RPT];
+    bool live[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        const uint32_t r = rl + j * it.tps;
+        live[j] = r < bk.nrows;
+        const RowMod m = mods[bk.row_begin + (live[j] ? r : 0)];
+#pragma unroll
+        for (int k = 0; k < L; ++k) n[j][k] = m.n[k];
+        ninv[j] = m.ninv;
+    }
+    const uint64_t T = bk.T;
+    uint64_t c0, c1;
+    split_range(bk, s, &c0, &c1);
+    Res<L> P[RPT], A[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) { set_small<L>(P[j], 1); set_small<L>(A[j], 1); }
+    u128 def = 0;
+    if (c0 < c1) {
+        uint64_t e_cur = T / cols[c0];
+        uint64_t thr = T / e_cur;
+        uint64_t cells = 0;
+        const uint64_t* cp = cols + c0;
+        const uint64_t* const ce = cols + c1;
+        while (cp < ce) {
+            if ((((uintptr_t)cp) & 31) == 0 && cp + 4 <= ce) {
+                const ulonglong2 g0 = __ldg(reinterpret_cast<const ulonglong2*>(cp));
+                const ulonglong2 g1 = __ldg(reinterpret_cast<const ulonglong2*>(cp) + 1);
+                if (g1.y <= thr) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        cell64<L>(P[j], g0.x, n[j], ninv[j]);
+                        cell64<L>(P[j], g0.y, n[j], ninv[j]);
+                        cell64<L>(P[j], g1.x, n[j], ninv[j]);
+                        cell64<L>(P[j], g1.y, n[j], ninv[j]);
+                    }
+                    cp += 4;
+                    cells += 4;
+                    continue;
+                }
+            }
+            const uint64_t q = __ldg(cp);
+            if (q > thr) {
+                const uint64_t e_new = T / q;
+                const uint64_t d = e_cur - e_new;
+                if (d) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
+                    def += (u128)d * (64 * cells + 32 * L);
+                }
+                e_cur = e_new;
+                thr = T / e_new;
+            }
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) cell64<L>(P[j], q, n[j], ninv[j]);
+            ++cp;
+            ++cells;
+        }
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], e_cur, n[j], ninv[j]);
+        def += (u128)e_cur * (64 * cells + 32 * L);
+    }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        if (!live[j]) continue;
+        const uint32_t r = rl + j * it.tps;
+        uint4 o;
+        o.x = A[j].w[0];
+        o.y = A[j].w[1];
+        o.z = L > 2 ? A[j].w[2 < L ? 2 : 0] : 0;
+        o.w = L > 3 ? A[j].w[3 < L ? 3 : 0] : 0;
+        part[bk.part_base + (uint64_t)s * bk.nrows + r] = o;
+    }
+    if (it.row0 == 0 && threadIdx.x % it.tps == 0) {
+        Deficit dd;
+        dd.lo = (uint64_t)def;
+        dd.hi = (uint64_t)(def >> 64);
+        defs[bk.def_base + s] = dd;
+    }
+}
+
+// acc[row] *= prod over the window's splits; the bucket's first row also
+// adds the splits' deficits (and 2^(32L) per product) into bdef[bucket]
+template <int L>
+__global__ void __launch_bounds__(128)
+k_merge(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
+        const uint4* __restrict__ part, const Deficit* __restrict__ defs, uint32_t row_begin, uint32_t nrows,
+        uint4* __restrict__ acc, Deficit* __restrict__ bdef) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const uint32_t row = row_begin + i;
+    const uint32_t b = info[row].bucket;
+    const Bucket bk = buckets[b];
+    if (bk.nsplit == 0) return;
+    const RowMod m = mods[row];
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    const uint32_t rl = row - bk.row_begin;
+    const uint4 a = acc[row];
+    Res<L> X;
+    X.w[0] = a.x; X.w[1] = a.y;
+    if (L > 2) X.w[2 < L ? 2 : 0] = a.z;
+    if (L > 3) X.w[3 < L ? 3 : 0] = a.w;
+    for (uint32_t s = 0; s < bk.nsplit; ++s) {
+        const uint4 v = part[bk.part_base + (uint64_t)s * bk.nrows + rl];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, m.ninv);
+    }
+    uint4 o;
+    o.x = X.w[0];
+    o.y = X.w[1];
+    o.z = L > 2 ? X.w[2 < L ? 2 : 0] : 0;
+    o.w = L > 3 ? X.w[3 < L ? 3 : 0] : 0;
+    acc[row] = o;
+    if (rl == 0) {
+        u128 d = ((u128)bdef[b].hi << 64) | bdef[b].lo;
+        for (uint32_t s = 0; s < bk.nsplit; ++s) {
+            const Deficit x = defs[bk.def_base + s];
+            d += (((u128)x.hi << 64) | x.lo) + 32 * L;
+        }
+        bdef[b].lo = (uint64_t)d;
+        bdef[b].hi = (uint64_t)(d >> 64);
+    }
+}
+
+// ===========================================================================
 // launch wrappers
 // ===========================================================================
 
@@ -999,14 +1286,53 @@ void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const Row
     else if (L == 3) k_iterate<3><<<g, 256, 0, st>>>(buckets, info, mods, row_begin, nrows, item_begin, nitems, K, out);
     else k_iterate<4><<<g, 256, 0, st>>>(buckets, info, mods, row_begin, nrows, item_begin, nitems, K, out);
 }
-void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
-                   const Deficit* defs, uint64_t K, const uint4* ipart, uint32_t row_begin,
-                   uint32_t nrows, int full, RowOut* out, cudaStream_t st) {
+void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_t* base, uint32_t nbase,
+                      uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st) {
+    if (!nseg) return;
+    const size_t smem = (BIG_WORDS + PRE_TABLE) * sizeof(uint32_t);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_sieve_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    const uint32_t ncta = (nseg + spc - 1) / spc;
+    k_sieve_big<<<ncta, BIG_THREADS, smem, st>>>(lo, hi, nseg, spc, base, nbase, offsets, bitmap, seg_count);
+}
+void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,
+                        cudaStream_t st) {
+    if (!nseg) return;
+    k_compact_big<<<nseg, 1024, 0, st>>>(lo0, bitmap, offsets, out);
+}
+void launch_count_leq64(const uint64_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys, uint64_t* out,
+                        cudaStream_t st) {
+    if (!nkeys) return;
+    k_count_leq64<<<(nkeys + 127) / 128, 128, 0, st>>>(cols, ncols, keys, nkeys, out);
+}
+void launch_sweep64(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
+                    const uint64_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+    if (!nitems) return;
+#define WL_S64(LL, RR) k_sweep64<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs)
+    if (L == 2) { if (rpt == 2) WL_S64(2, 2); else WL_S64(2, 1); }
+    else if (L == 3) { if (rpt == 2) WL_S64(3, 2); else WL_S64(3, 1); }
+    else { if (rpt == 2) WL_S64(4, 2); else WL_S64(4, 1); }
+#undef WL_S64
+}
+void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                  const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st) {
     if (!nrows) return;
     const unsigned g = (nrows + 127) / 128;
-    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
-    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
-    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out);
+    if (L == 2) k_merge<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, row_begin, nrows, acc, bdef);
+    else if (L == 3) k_merge<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, row_begin, nrows, acc, bdef);
+    else k_merge<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, row_begin, nrows, acc, bdef);
+}
+void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                   const Deficit* defs, uint64_t K, const uint4* ipart, uint32_t row_begin,
+                   uint32_t nrows, int full, RowOut* out, cudaStream_t st, const uint4* bacc, const Deficit* bdef) {
+    if (!nrows) return;
+    const unsigned g = (nrows + 127) / 128;
+    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
+    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
+    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
 }
 
 }  // namespace wl

@@ -83,6 +83,8 @@ def lib():
         L.orc_count_primes_below.restype = ctypes.c_size_t
         L.orc_count_primes_below.argtypes = [u64]
         L.orc_threads.restype = ctypes.c_int
+        L.orc_range_product.restype = None
+        L.orc_range_product.argtypes = [u64, u64, u64, u64, ctypes.POINTER(u64), ctypes.POINTER(u64)]
         _lib = L
     return _lib
 
@@ -142,6 +144,13 @@ def factorial_mod_p2(p: int):
 def small_factorial(p: int, T: int):
     s0, s1 = ctypes.c_uint64(), ctypes.c_uint64()
     lib().orc_small_factorial(p, T, ctypes.byref(s0), ctypes.byref(s1))
+    return s0.value, s1.value
+
+
+def range_product(p: int, T: int, qlo: int, qhi: int):
+    """Digits of prod_{qlo <= q < qhi, q prime} q^{v_q(T!)} mod p^2."""
+    s0, s1 = ctypes.c_uint64(), ctypes.c_uint64()
+    lib().orc_range_product(p, T, qlo, qhi, ctypes.byref(s0), ctypes.byref(s1))
     return s0.value, s1.value
 
 

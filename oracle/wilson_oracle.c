@@ -687,3 +687,48 @@ int orc_threads(void) {
     return 1;
 #endif
 }
+
+/* Product over the primes q in [qlo, qhi) (qhi <= 2^40) of q^{v_q(T!)} mod p^2,
+   returned as digits (s0, s1): the contribution of one slice of the column
+   sweep (mullarge.cl:36-63 for q above 2^32, where v_q(T!) = floor(T/q) once
+   q > sqrt(T)).  Segmented sieve with 64-bit values. */
+void orc_range_product(u64 p, u64 T, u64 qlo, u64 qhi, u64 *s0, u64 *s1) {
+    tpconst c = setup_prime(p);
+    u64x2 res = c.one;
+    if (qhi > T + 1) qhi = T + 1;
+    if (qlo < 2) qlo = 2;
+    if (qlo < qhi) {
+        sieve_base b = make_base(qhi);
+        const u64 span = 1ULL << 24;
+        uint8_t *comp = (uint8_t *)malloc(span / 2 + 2);
+        for (u64 lo = qlo; lo < qhi; lo += span) {
+            u64 hi = lo + span < qhi ? lo + span : qhi;
+            if (lo <= 2 && 2 < hi) {
+                u64 e, cb; get_power(2, T, &e, &cb);
+                res = m2p_mul(res, m2p_pow(&c, to_mont(&c, 2), e), c.p, c.q);
+            }
+            u64 first = lo | 1;
+            if (first >= hi) continue;
+            u64 nodd = (hi - first + 1) / 2;
+            memset(comp, 0, nodd);
+            for (size_t k = 0; k < b.n; ++k) {
+                u64 q = b.p[k];
+                if (q * q >= hi) break;
+                u64 m = (first + q - 1) / q * q;
+                if (m < q * q) m = q * q;
+                if (!(m & 1)) m += q;
+                for (u64 j = (m - first) / 2; j < nodd; j += q) comp[j] = 1;
+            }
+            for (u64 j = 0; j < nodd; ++j) {
+                u64 v = first + 2 * j;
+                if (comp[j] || v < 3) continue;
+                u64 e, cb; get_power(v, T, &e, &cb);
+                res = m2p_mul(res, m2p_pow(&c, to_mont(&c, v), e), c.p, c.q);
+            }
+        }
+        free(comp);
+        free(b.p);
+    }
+    u64x2 v = m2p_get(res, c.p, c.q);
+    *s0 = v.s0; *s1 = v.s1;
+}

@@ -158,3 +158,37 @@ def test_errors(engine):
     with pytest.raises(wl.WilsonError) as e:
         engine.search(24, 29)            # no primes in [24, 29)
     assert e.value.code == -3
+
+
+def _range_oracle(args):
+    p, T, lo, hi = args
+    return oracle.range_product(p, T, lo, hi)
+
+
+@pytest.mark.parametrize("lo,hi,nsample", [(10**13, 10**13 + 20000, 8), ((1 << 62) - 20001, (1 << 62) - 1, 4)])
+def test_big_columns_against_oracle(engine, lo, hi, nsample):
+    # capped(2^32 + 2^26) = capped(2^32) * prod_{2^32 <= q < 2^32 + 2^26} q^{v_q(T!)}:
+    # the window sieve, the 64-bit sweep and the merge against the oracle
+    from concurrent.futures import ThreadPoolExecutor
+    q1, q2 = 1 << 32, (1 << 32) + (1 << 26)
+    r1, st = engine.rows(lo, hi, q_cap=q1)
+    r2, _ = engine.rows(lo, hi, q_cap=q2)
+    idx = list(range(0, len(r1), max(1, len(r1) // nsample)))[:nsample]
+    jobs = [(int(r1["p"][i]), st.targets[int(r1["type"][i])], q1, q2) for i in idx]
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        parts = list(ex.map(_range_oracle, jobs))
+    for i, (s0, s1) in zip(idx, parts):
+        p = int(r1["p"][i])
+        m = p * p
+        a = int(r1["s0"][i]) + p * int(r1["s1"][i])
+        b = int(r2["s0"][i]) + p * int(r2["s1"][i])
+        assert a * (s0 + p * s1) % m == b, p
+
+
+def test_kat1_columns_above_2_32(engine, golden):
+    # self-test case 1: class target 2.07e11, columns up to it (cl_wilson.cpp:2007-2013)
+    k = golden["kat"][0]
+    res = engine.search(k["pmin"], k["pmax"])
+    assert res.stats.pi_maxtarget == k["pi_maxtarget"]
+    assert "%016X" % res.checksum == k["checksum"]
+    assert res.results == [(k["last_prime"], k["last_value"])]

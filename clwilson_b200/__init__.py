@@ -66,7 +66,7 @@ class _Stats(ctypes.Structure):
                 ("checksum", ctypes.c_uint64), ("results", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
                 ("ms_device", ctypes.c_double), ("ms_primes", ctypes.c_double), ("ms_sieve", ctypes.c_double),
                 ("ms_sweep", ctypes.c_double), ("ms_iterate", ctypes.c_double), ("ms_finish", ctypes.c_double),
-                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double)]
 
 
 ROW_DTYPE = np.dtype([("p", "<u8"), ("s0", "<u8"), ("s1", "<u8"), ("rem", "<u8"), ("quot", "<u8"),
@@ -160,12 +160,13 @@ class Stats:
     ms_finish: float = 0.0
     h2d_bytes: int = 0
     d2h_bytes: int = 0
+    ms_big: float = 0.0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.tested, tuple(s.per_class), tuple(s.targets), s.pi_maxtarget, s.cells, s.tail_steps,
                    s.checksum, s.results, s.kernel_launches, s.ms_device, s.ms_primes, s.ms_sieve, s.ms_sweep,
-                   s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes)
+                   s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes, s.ms_big)
 
 
 @dataclass

@@ -117,6 +117,9 @@ struct wl_ctx {
     cudaStream_t st2 = nullptr;   // dense sweep, overlapped with the sparse sweep
     cudaEvent_t ev[8] = {};
     cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t big0 = nullptr, big1 = nullptr;
+    cudaEvent_t rows_ready = nullptr;   // row tables uploaded and k_setup_rows done (main stream)
+    double ms_big = 0;
     DevBuf base;            // odd primes < 65536 (sieving primes of the column sieve)
     uint32_t nbase = 0;
     DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
@@ -126,6 +129,7 @@ struct wl_ctx {
     // columns above 2^32
     cudaStream_t st3 = nullptr;
     DevBuf bbitmap, bsegcount, boffsets, boffs, wcols, wbuckets, witems, wpart, wdefs, bacc, bdef, wkeys, wcounts;
+    DevBuf uacc, udef;   // columns below 2^32: per-row product of all splits, per-bucket deficit
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
@@ -214,6 +218,8 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
                            uint64_t qcap, uint64_t* pi_big) {
     (void)keys_host_order;
     cudaStream_t s3 = c->st3;
+    CK(cudaStreamWaitEvent(s3, c->rows_ready, 0));   // row tables and moduli
+    CK(cudaEventRecord(c->big0, s3));
     const uint64_t LO = 1ull << 32;
     const uint64_t WIN = 1ull << 33;
     const uint32_t SPC = 8;
@@ -243,12 +249,8 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
     // running per-row accumulators (raw 1) and per-bucket deficits (0)
     RC(ensure(c->bacc, (size_t)nrows * 16 + 16));
     RC(ensure(c->bdef, db.size() * sizeof(Deficit) + 16));
-    {
-        std::vector<uint4> ones(nrows, make_uint4(1, 0, 0, 0));
-        CK(cudaMemcpyAsync(c->bacc.p, ones.data(), (size_t)nrows * 16, cudaMemcpyHostToDevice, s3));
-        CK(cudaMemsetAsync(c->bdef.p, 0, db.size() * sizeof(Deficit), s3));
-        CK(cudaStreamSynchronize(s3));   // `ones` goes out of scope
-    }
+    launch_acc_init(nrows, (uint32_t)db.size(), as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
+    c->launches++;
     // row groups by limb width (rows are ordered by width)
     std::vector<std::pair<int, std::pair<uint32_t, uint32_t>>> lgroups;
     for (uint32_t rb = 0; rb < nrows;) {
@@ -260,72 +262,60 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
     }
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
     *pi_big = 0;
+    // device: per-bucket keys for the bitmap sweep, the pi(maxtarget) counter
+    RC(ensure(c->wkeys, db.size() * 8 + 16));
+    RC(ensure(c->wcounts, 16));
+    CK(cudaMemcpyAsync(c->wkeys.p, bkey.data(), db.size() * 8, cudaMemcpyHostToDevice, s3));
+    CK(cudaMemsetAsync(c->wcounts.p, 0, 8, s3));
+    std::vector<Bucket> wb(db);
+    std::vector<SweepItem> all;
     for (uint64_t w0 = LO; w0 < big_need; w0 += WIN) {
         const uint64_t w1 = std::min(w0 + WIN, big_need);
         const uint32_t nseg = (uint32_t)((w1 - w0 + BIG_SPAN - 1) / BIG_SPAN);
         const uint32_t ncta = (nseg + SPC - 1) / SPC;
         RC(ensure(c->bbitmap, (size_t)nseg * BIG_WORDS * 4));
         RC(ensure(c->bsegcount, (size_t)nseg * 4));
-        RC(ensure(c->boffsets, (size_t)(nseg + 1) * 8));
         RC(ensure(c->boffs, (size_t)ncta * std::max<uint32_t>(nbase, 1) * 4));
         launch_sieve_big(w0, w1, nseg, SPC, base, nbase, as<uint32_t>(c->boffs), as<uint32_t>(c->bbitmap),
                          as<uint32_t>(c->bsegcount), s3);
         c->launches++;
-        std::vector<uint32_t> segcnt(nseg);
-        CK(cudaMemcpyAsync(segcnt.data(), c->bsegcount.p, (size_t)nseg * 4, cudaMemcpyDeviceToHost, s3));
-        CK(cudaStreamSynchronize(s3));
-        CK(cudaGetLastError());
-        std::vector<uint64_t> offs(nseg + 1);
-        uint64_t tot = 0;
-        for (uint32_t k = 0; k < nseg; ++k) { offs[k] = tot; tot += segcnt[k]; }
-        offs[nseg] = tot;
-        if (tot == 0) continue;
-        RC(ensure(c->wcols, tot * 8 + 64));
-        CK(cudaMemcpyAsync(c->boffsets.p, offs.data(), (size_t)(nseg + 1) * 8, cudaMemcpyHostToDevice, s3));
-        launch_compact_big(nseg, w0, as<uint32_t>(c->bbitmap), as<uint64_t>(c->boffsets), as<uint64_t>(c->wcols), s3);
-        c->launches++;
-        // columns of the window per bucket (<= its key), and <= maxt0 for pi(maxtarget)
-        std::vector<uint64_t> wk(db.size() + 1);
-        for (size_t b = 0; b < db.size(); ++b) wk[b] = bkey[b] >= w0 ? std::min(bkey[b], w1 - 1) : 0;
-        wk[db.size()] = maxt0;
-        RC(ensure(c->wkeys, wk.size() * 8));
-        RC(ensure(c->wcounts, wk.size() * 8));
-        CK(cudaMemcpyAsync(c->wkeys.p, wk.data(), wk.size() * 8, cudaMemcpyHostToDevice, s3));
-        launch_count_leq64(as<uint64_t>(c->wcols), tot, as<uint64_t>(c->wkeys), (uint32_t)wk.size(),
-                           as<uint64_t>(c->wcounts), s3);
-        c->launches++;
-        std::vector<uint64_t> wn(wk.size());
-        CK(cudaMemcpyAsync(wn.data(), c->wcounts.p, wk.size() * 8, cudaMemcpyDeviceToHost, s3));
-        CK(cudaStreamSynchronize(s3));
-        CK(cudaGetLastError());
-        *pi_big += wn[db.size()];
-        // window buckets and sweep items
-        std::vector<Bucket> wb(db);
+        if (maxt0 >= w0) {
+            launch_count_bits(as<uint32_t>(c->bbitmap), w0, (uint64_t)nseg * BIG_WORDS, maxt0,
+                              as<unsigned long long>(c->wcounts), s3);
+            c->launches++;
+        }
+        // window buckets: the words covering w0 .. min(key, w1 - 1), split by work
         double W = 0;
+        std::vector<uint64_t> nw(db.size(), 0);
         for (size_t b = 0; b < db.size(); ++b) {
-            if (bkey[b] < w0) wn[b] = 0;
-            W += (double)db[b].nrows * (double)wn[b];
+            if (bkey[b] < w0) continue;
+            const uint64_t top = std::min(bkey[b], w1 - 1);
+            nw[b] = (top - w0) / 64 + 1;
+            W += (double)db[b].nrows * (double)nw[b];
         }
         if (W == 0) continue;
         struct Grp { int L, rpt; std::vector<SweepItem> items; };
         std::vector<Grp> groups;
         uint64_t part_total = 0;
         uint32_t def_total = 0;
+        uint32_t maxs = 0;
         for (size_t b = 0; b < db.size(); ++b) {
             Bucket& x = wb[b];
-            x.ncols = (uint32_t)wn[b];
+            x = db[b];
+            x.ncols = (uint32_t)nw[b];
             x.cdense = 0;
             x.ndense = 0;
             x.part_base = part_total;
             x.def_base = def_total;
-            if (!wn[b]) { x.nsplit = 0; continue; }
+            if (!nw[b]) { x.nsplit = 0; continue; }
             int rpt, tps;
             if (x.nrows >= 512) { rpt = 2; tps = 256; }
             else if (x.nrows >= 256) { rpt = 1; tps = 256; }
             else { rpt = 1; tps = 1; while (tps < (int)x.nrows) tps <<= 1; }
-            uint64_t S = (uint64_t)std::ceil((double)rpt * (double)wn[b] * target_threads / W);
-            S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, wn[b] / 2048)));
+            uint64_t S = (uint64_t)std::ceil((double)rpt * (double)nw[b] * target_threads / W);
+            S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, nw[b] / 256)));
             x.nsplit = (uint32_t)S;
+            maxs = std::max<uint32_t>(maxs, x.nsplit);
             part_total += S * x.nrows;
             def_total += (uint32_t)S;
             Grp* g = nullptr;
@@ -339,7 +329,10 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
                 for (uint32_t s2 = 0; s2 < S; s2 += per) g->items.push_back({ (uint32_t)b, 0, s2, (uint32_t)tps });
             }
         }
-        std::vector<SweepItem> all;
+        // the previous window's copies must be done before these host vectors change
+        CK(cudaStreamSynchronize(s3));
+        CK(cudaGetLastError());
+        all.clear();
         for (auto& g : groups) all.insert(all.end(), g.items.begin(), g.items.end());
         RC(ensure(c->wbuckets, wb.size() * sizeof(Bucket)));
         RC(ensure(c->witems, all.size() * sizeof(SweepItem) + 16));
@@ -349,24 +342,38 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
         CK(cudaMemcpyAsync(c->witems.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, s3));
         size_t ioff = 0;
         for (auto& g : groups) {
-            launch_sweep64(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->wbuckets),
-                           as<SweepItem>(c->witems) + ioff, as<RowMod>(c->rowmod), as<uint64_t>(c->wcols),
-                           as<uint4>(c->wpart), as<Deficit>(c->wdefs), s3);
+            launch_sweep_bits(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->wbuckets),
+                              as<SweepItem>(c->witems) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->bbitmap), w0,
+                              as<uint64_t>(c->wkeys), as<uint4>(c->wpart), as<Deficit>(c->wdefs), s3);
             c->launches++;
             ioff += g.items.size();
         }
         for (auto& g : lgroups) {
-            launch_merge(g.first, as<Bucket>(c->wbuckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
-                         as<uint4>(c->wpart), as<Deficit>(c->wdefs), g.second.first, g.second.second - g.second.first,
-                         as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
+            if (maxs >= 64)
+                launch_merge_cta(g.first, as<Bucket>(c->wbuckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                                 as<uint4>(c->wpart), as<Deficit>(c->wdefs), g.second.first,
+                                 g.second.second - g.second.first, as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
+            else
+                launch_merge(g.first, as<Bucket>(c->wbuckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                             as<uint4>(c->wpart), as<Deficit>(c->wdefs), g.second.first, g.second.second - g.second.first,
+                             as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
             c->launches++;
         }
-        // host vectors above are consumed by queued copies: wait before reuse
+    }
+    {
+        unsigned long long pi = 0;
+        CK(cudaMemcpyAsync(&pi, c->wcounts.p, 8, cudaMemcpyDeviceToHost, s3));
         CK(cudaStreamSynchronize(s3));
         CK(cudaGetLastError());
+        *pi_big = pi;
     }
+    CK(cudaEventRecord(c->big1, s3));
     CK(cudaEventRecord(c->join, s3));
     CK(cudaStreamWaitEvent(c->st, c->join, 0));
+    CK(cudaEventSynchronize(c->big1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->big0, c->big1);
+    c->ms_big = ms;
     return 0;
 }
 
@@ -375,6 +382,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     c->launches = 0;
     c->h2d = c->d2h = 0;
     c->ms_sieve = 0;
+    c->ms_big = 0;
     for (size_t i = 0; i < nr; ++i) RC(wl_check_range(ranges[i].pmin, ranges[i].pmax));
 
     cudaEventRecord(c->ev[0], c->st);
@@ -713,6 +721,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
 
     launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
     c->launches++;
+    CK(cudaEventRecord(c->rows_ready, c->st));
     cudaEventRecord(c->ev[2], c->st);
     size_t ioff = 0;
     bool forked = false;
@@ -736,6 +745,30 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     if (forked) {
         CK(cudaEventRecord(c->join, c->st2));
         CK(cudaStreamWaitEvent(c->st, c->join, 0));
+    }
+    // merge every row's split partials into its accumulator
+    RC(ensure(c->uacc, (size_t)nrows * 16 + 16));
+    RC(ensure(c->udef, db.size() * sizeof(Deficit) + 16));
+    launch_acc_init(nrows, (uint32_t)db.size(), as<uint4>(c->uacc), as<Deficit>(c->udef), c->st);
+    c->launches++;
+    {
+        uint32_t maxs = 0;
+        for (auto& x : db) maxs = std::max(maxs, x.nsplit);
+        for (uint32_t rb = 0; rb < nrows;) {
+            const int L = (int)db[ri[rb].bucket].L;
+            uint32_t re = rb;
+            while (re < nrows && (int)db[ri[re].bucket].L == L) ++re;
+            if (maxs >= 64)
+                launch_merge_cta(L, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                                 as<uint4>(c->part), as<Deficit>(c->defs), rb, re - rb, as<uint4>(c->uacc),
+                                 as<Deficit>(c->udef), c->st);
+            else
+                launch_merge(L, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
+                             as<uint4>(c->part), as<Deficit>(c->defs), rb, re - rb, as<uint4>(c->uacc),
+                             as<Deficit>(c->udef), c->st);
+            c->launches++;
+            rb = re;
+        }
     }
     bool big = false;
     if (big_need) {
@@ -771,7 +804,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         launch_finish(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
                       as<uint4>(c->part), as<Deficit>(c->defs), K, as<uint4>(c->ipart),
                       g.second.first, g.second.second - g.second.first, full ? 1 : 0, as<RowOut>(c->rowout), c->st,
-                      big ? as<uint4>(c->bacc) : nullptr, big ? as<Deficit>(c->bdef) : nullptr);
+                      as<uint4>(c->uacc), as<Deficit>(c->udef), big ? as<uint4>(c->bacc) : nullptr,
+                      big ? as<Deficit>(c->bdef) : nullptr);
         c->launches++;
     }
     std::vector<RowOut> ro(nrows);
@@ -820,6 +854,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         st->kernel_launches = c->launches;
         st->h2d_bytes = c->h2d;
         st->d2h_bytes = c->d2h;
+        st->ms_big = c->ms_big;
     }
     return 0;
 }
@@ -929,6 +964,9 @@ int wl_open(int device, wl_ctx** out) {
     for (auto& e : c->ev) cudaEventCreate(&e);
     cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
+    cudaEventCreate(&c->big0);
+    cudaEventCreateWithFlags(&c->rows_ready, cudaEventDisableTiming);
+    cudaEventCreate(&c->big1);
     // odd primes below 2^16: the sieving primes of the column sieve (q < 2^32)
     std::vector<uint8_t> comp(65536, 0);
     std::vector<uint32_t> base;
@@ -953,12 +991,15 @@ void wl_close(wl_ctx* c) {
     DevBuf* bufs[] = { &c->base, &c->cols, &c->bitmap, &c->segcount, &c->offsets, &c->tp, &c->keys, &c->counts,
                        &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
                        &c->bbitmap, &c->bsegcount, &c->boffsets, &c->boffs, &c->wcols, &c->wbuckets, &c->witems,
-                       &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts,
+                       &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts, &c->uacc, &c->udef,
                        &c->defs, &c->rowout };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->fork) cudaEventDestroy(c->fork);
     if (c->join) cudaEventDestroy(c->join);
+    if (c->big0) cudaEventDestroy(c->big0);
+    if (c->rows_ready) cudaEventDestroy(c->rows_ready);
+    if (c->big1) cudaEventDestroy(c->big1);
     if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st3) cudaStreamDestroy(c->st3);
     if (c->st) cudaStreamDestroy(c->st);

@@ -116,13 +116,23 @@ void launch_count_leq64(const uint64_t* cols, uint64_t ncols, const uint64_t* ke
                         cudaStream_t st);
 void launch_sweep64(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
                     const uint64_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_sweep_bits(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                       const RowMod* mods, const uint32_t* bitmap, uint64_t lo, const uint64_t* keys, uint4* part,
+                       Deficit* defs, cudaStream_t st);
+void launch_count_bits(const uint32_t* bitmap, uint64_t lo, uint64_t nwords, uint64_t key, unsigned long long* out,
+                       cudaStream_t st);
 void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
                   const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
+void launch_acc_init(uint32_t nrows, uint32_t nbuckets, uint4* acc, Deficit* bdef, cudaStream_t st);
+void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                      const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef,
+                      cudaStream_t st);
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
                     uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st);
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods,
                    const uint4* part, const Deficit* defs, uint64_t K, const uint4* ipart,
                    uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st,
-                   const uint4* bacc = nullptr, const Deficit* bdef = nullptr);
+                   const uint4* acc1 = nullptr, const Deficit* def1 = nullptr,
+                   const uint4* acc2 = nullptr, const Deficit* def2 = nullptr);
 
 }  // namespace wl

@@ -796,7 +796,8 @@ __global__ void __launch_bounds__(128)
 k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
          const uint4* __restrict__ part, const Deficit* __restrict__ defs, uint64_t K,
          const uint4* __restrict__ ipart, uint32_t row_begin, uint32_t nrows, int full,
-         RowOut* __restrict__ out, const uint4* __restrict__ bacc, const Deficit* __restrict__ bdef) {
+         RowOut* __restrict__ out, const uint4* __restrict__ acc1, const Deficit* __restrict__ def1,
+         const uint4* __restrict__ acc2, const Deficit* __restrict__ def2, int merged) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrows) return;
     const uint32_t row = row_begin + i;
@@ -813,7 +814,7 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
     Res<L> X;
     set_small<L>(X, 1);
     u128 def = 0;
-    for (uint32_t s = 0; s < bk.nsplit; ++s) {
+    for (uint32_t s = 0; s < (merged ? 0u : bk.nsplit); ++s) {
         const uint4 v = part[bk.part_base + (uint64_t)s * bk.nrows + rl];
         Res<L> y;
         y.w[0] = v.x; y.w[1] = v.y;
@@ -838,15 +839,19 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
         const bool small = start + len - 1 < 0x80000000ull;
         def += (u128)len * (small ? 32 : 64) + 32 * L;
     }
-    // columns above 2^32, merged window by window
-    if (bacc) {
-        const uint4 v = bacc[row];
+    // split partials merged into per-row accumulators (k_merge*): columns
+    // below 2^32 and, when used, the windows above
+    for (int a = 0; a < 2; ++a) {
+        const uint4* acc = a ? acc2 : acc1;
+        const Deficit* dd = a ? def2 : def1;
+        if (!acc) continue;
+        const uint4 v = acc[row];
         Res<L> y;
         y.w[0] = v.x; y.w[1] = v.y;
         if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
         if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
         X = mont_mul<L>(X, y, n, ninv);
-        const Deficit d = bdef[ri.bucket];
+        const Deficit d = dd[ri.bucket];
         def += (((u128)d.hi << 64) | d.lo) + 32 * L;
     }
     // R mod n (Montgomery one), 2R mod n, R^2 mod n by doubling
@@ -962,6 +967,8 @@ k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_
     uint32_t* bm = smem;                  // BIG_WORDS words
     uint32_t* tab = smem + BIG_WORDS;     // PRE_TABLE masks
     __shared__ uint32_t wsum[BIG_THREADS / 32];
+    __shared__ uint32_t sres[BIG_PRESIEVE], sinc[BIG_PRESIEVE];
+    if (threadIdx.x < BIG_PRESIEVE) sinc[threadIdx.x] = (64u * blockDim.x) % c_pre[threadIdx.x];
     for (uint32_t i = threadIdx.x; i < PRE_TABLE; i += blockDim.x) {
         uint32_t j = 0;
         while (j + 1 < BIG_PRESIEVE && c_preoff[j + 1] <= i) ++j;
@@ -988,11 +995,24 @@ k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_
         const uint32_t seg = seg0 + j;
         if (seg >= nseg) break;                          // uniform across the CTA
         const uint64_t slo = cta_lo + (uint64_t)j * BIG_SPAN;
+        // residues of the thread's first word start, then stepped by
+        // blockDim.x words (64 * blockDim.x integers) with an add and a subtract
+        if (threadIdx.x < BIG_PRESIEVE) sres[threadIdx.x] = (uint32_t)(slo % c_pre[threadIdx.x]);
+        __syncthreads();
+        uint32_t rr[BIG_PRESIEVE];
+#pragma unroll
+        for (uint32_t q = 0; q < BIG_PRESIEVE; ++q) {
+            const uint32_t p = c_pre[q];
+            rr[q] = (sres[q] + (64u * threadIdx.x + 1u) % p) % p;
+        }
         for (uint32_t w = threadIdx.x; w < BIG_WORDS; w += blockDim.x) {
-            const uint64_t n0 = slo + 64ull * w + 1;
             uint32_t word = 0;
 #pragma unroll
-            for (uint32_t q = 0; q < BIG_PRESIEVE; ++q) word |= tab[c_preoff[q] + (uint32_t)(n0 % c_pre[q])];
+            for (uint32_t q = 0; q < BIG_PRESIEVE; ++q) {
+                word |= tab[c_preoff[q] + rr[q]];
+                rr[q] += sinc[q];
+                if (rr[q] >= c_pre[q]) rr[q] -= c_pre[q];
+            }
             bm[w] = word;
         }
         __syncthreads();
@@ -1168,6 +1188,111 @@ k_sweep64(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ item
     }
 }
 
+// Sweep straight from a window's sieve bitmap: word w holds the odd numbers
+// lo + 64w + 1 + 2b (bit b).  Bucket fields for the window: ncols = words used,
+// split s = words [ncols*s/nsplit, ncols*(s+1)/nsplit); primes above `key`
+// (the bucket's target or q_cap - 1) are skipped.  Otherwise as k_sweep64.
+template <int L, int RPT>
+__global__ void __launch_bounds__(256)
+k_sweep_bits(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
+             const uint32_t* __restrict__ bitmap, uint64_t lo, const uint64_t* __restrict__ keys,
+             uint4* __restrict__ part, Deficit* __restrict__ defs) {
+    const SweepItem it = items[blockIdx.x];
+    const Bucket bk = buckets[it.bucket];
+    const uint32_t s = it.split0 + threadIdx.x / it.tps;
+    if (s >= bk.nsplit) return;
+    const uint32_t rl = it.row0 + threadIdx.x % it.tps;
+    uint32_t n[RPT][L];
+    uint32_t ninv[RPT];
+    bool live[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        const uint32_t r = rl + j * it.tps;
+        live[j] = r < bk.nrows;
+        const RowMod m = mods[bk.row_begin + (live[j] ? r : 0)];
+#pragma unroll
+        for (int k = 0; k < L; ++k) n[j][k] = m.n[k];
+        ninv[j] = m.ninv;
+    }
+    const uint64_t T = bk.T, key = keys[it.bucket];
+    const uint64_t w0 = (uint64_t)bk.ncols * s / bk.nsplit;
+    const uint64_t w1 = (uint64_t)bk.ncols * (s + 1) / bk.nsplit;
+    Res<L> P[RPT], A[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) { set_small<L>(P[j], 1); set_small<L>(A[j], 1); }
+    u128 def = 0;
+    uint64_t e_cur = 0, thr = 0, cells = 0;
+    bool started = false;
+    for (uint64_t w = w0; w < w1; ++w) {
+        uint32_t word = __ldg(bitmap + w);
+        const uint64_t qb = lo + 64 * w + 1;
+        while (word) {
+            const int b = __ffs(word) - 1;
+            word &= word - 1;
+            const uint64_t q = qb + 2ull * b;
+            if (q > key) { w = w1; break; }
+            if (!started) {
+                started = true;
+                e_cur = T / q;
+                thr = T / e_cur;
+            } else if (q > thr) {
+                const uint64_t e_new = T / q;
+                const uint64_t d = e_cur - e_new;
+                if (d) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
+                    def += (u128)d * (64 * cells + 32 * L);
+                }
+                e_cur = e_new;
+                thr = T / e_new;
+            }
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) cell64<L>(P[j], q, n[j], ninv[j]);
+            ++cells;
+        }
+    }
+    if (started) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], e_cur, n[j], ninv[j]);
+        def += (u128)e_cur * (64 * cells + 32 * L);
+    }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        if (!live[j]) continue;
+        const uint32_t r = rl + j * it.tps;
+        uint4 o;
+        o.x = A[j].w[0];
+        o.y = A[j].w[1];
+        o.z = L > 2 ? A[j].w[2 < L ? 2 : 0] : 0;
+        o.w = L > 3 ? A[j].w[3 < L ? 3 : 0] : 0;
+        part[bk.part_base + (uint64_t)s * bk.nrows + r] = o;
+    }
+    if (it.row0 == 0 && threadIdx.x % it.tps == 0) {
+        Deficit dd;
+        dd.lo = (uint64_t)def;
+        dd.hi = (uint64_t)(def >> 64);
+        defs[bk.def_base + s] = dd;
+    }
+}
+
+// number of set bits of a window bitmap standing for numbers <= key
+__global__ void k_count_bits(const uint32_t* __restrict__ bitmap, uint64_t lo, uint64_t nwords, uint64_t key,
+                             unsigned long long* __restrict__ out) {
+    uint32_t c = 0;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t first = lo + 64 * w + 1;
+        if (first > key) continue;
+        uint32_t word = bitmap[w];
+        if (first + 62 > key) {
+            const uint32_t keep_bits = (uint32_t)((key - first) / 2 + 1);   // bits 0 .. keep_bits-1
+            word &= keep_bits >= 32 ? ~0u : ((1u << keep_bits) - 1);
+        }
+        c += __popc(word);
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
 // acc[row] *= prod over the window's splits; the bucket's first row also
 // adds the splits' deficits (and 2^(32L) per product) into bdef[bucket]
 template <int L>
@@ -1213,6 +1338,81 @@ k_merge(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, co
         }
         bdef[b].lo = (uint64_t)d;
         bdef[b].hi = (uint64_t)(d >> 64);
+    }
+}
+
+__global__ void k_acc_init(uint32_t nrows, uint32_t nbuckets, uint4* __restrict__ acc, Deficit* __restrict__ bdef) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nrows) acc[i] = make_uint4(1, 0, 0, 0);
+    if (i < nbuckets) { bdef[i].lo = 0; bdef[i].hi = 0; }
+}
+
+// acc[row] *= prod of the row's split partials, one CTA per row: strided
+// products per thread, then a product tree in shared memory.  Deficit of the
+// product: the splits' deficits + 2^(32L) for each of the nsplit + 256
+// Montgomery products (nsplit strided, 255 tree, 1 into acc); row 0's CTA adds
+// it to bdef[bucket].
+template <int L>
+__global__ void __launch_bounds__(256)
+k_merge_cta(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
+            const uint4* __restrict__ part, const Deficit* __restrict__ defs, uint32_t row_begin,
+            uint4* __restrict__ acc, Deficit* __restrict__ bdef) {
+    __shared__ uint4 sx[256];
+    __shared__ u128 sd[256];
+    const uint32_t row = row_begin + blockIdx.x;
+    const uint32_t b = info[row].bucket;
+    const Bucket bk = buckets[b];
+    if (bk.nsplit == 0) return;                      // uniform across the CTA
+    const RowMod m = mods[row];
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    const uint32_t rl = row - bk.row_begin;
+    Res<L> X;
+    set_small<L>(X, 1);
+    u128 d = 0;
+    for (uint32_t s = threadIdx.x; s < bk.nsplit; s += blockDim.x) {
+        const uint4 v = part[bk.part_base + (uint64_t)s * bk.nrows + rl];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, m.ninv);
+        if (rl == 0) {
+            const Deficit x = defs[bk.def_base + s];
+            d += ((u128)x.hi << 64) | x.lo;
+        }
+    }
+    sx[threadIdx.x] = make_uint4(X.w[0], X.w[1], L > 2 ? X.w[2 < L ? 2 : 0] : 0, L > 3 ? X.w[3 < L ? 3 : 0] : 0);
+    sd[threadIdx.x] = d;
+    __syncthreads();
+    for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            const uint4 a = sx[threadIdx.x], c = sx[threadIdx.x + h];
+            Res<L> A, C;
+            A.w[0] = a.x; A.w[1] = a.y; C.w[0] = c.x; C.w[1] = c.y;
+            if (L > 2) { A.w[2 < L ? 2 : 0] = a.z; C.w[2 < L ? 2 : 0] = c.z; }
+            if (L > 3) { A.w[3 < L ? 3 : 0] = a.w; C.w[3 < L ? 3 : 0] = c.w; }
+            A = mont_mul<L>(A, C, n, m.ninv);
+            sx[threadIdx.x] = make_uint4(A.w[0], A.w[1], L > 2 ? A.w[2 < L ? 2 : 0] : 0, L > 3 ? A.w[3 < L ? 3 : 0] : 0);
+            sd[threadIdx.x] += sd[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint4 a = acc[row], t = sx[0];
+        Res<L> A, C;
+        A.w[0] = a.x; A.w[1] = a.y; C.w[0] = t.x; C.w[1] = t.y;
+        if (L > 2) { A.w[2 < L ? 2 : 0] = a.z; C.w[2 < L ? 2 : 0] = t.z; }
+        if (L > 3) { A.w[3 < L ? 3 : 0] = a.w; C.w[3 < L ? 3 : 0] = t.w; }
+        A = mont_mul<L>(A, C, n, m.ninv);
+        acc[row] = make_uint4(A.w[0], A.w[1], L > 2 ? A.w[2 < L ? 2 : 0] : 0, L > 3 ? A.w[3 < L ? 3 : 0] : 0);
+        if (rl == 0) {
+            u128 tot = ((u128)bdef[b].hi << 64) | bdef[b].lo;
+            tot += sd[0] + (u128)32 * L * ((u128)bk.nsplit + blockDim.x);
+            bdef[b].lo = (uint64_t)tot;
+            bdef[b].hi = (uint64_t)(tot >> 64);
+        }
     }
 }
 
@@ -1290,11 +1490,7 @@ void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, con
                       uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st) {
     if (!nseg) return;
     const size_t smem = (BIG_WORDS + PRE_TABLE) * sizeof(uint32_t);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_sieve_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    cudaFuncSetAttribute(k_sieve_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const uint32_t ncta = (nseg + spc - 1) / spc;
     k_sieve_big<<<ncta, BIG_THREADS, smem, st>>>(lo, hi, nseg, spc, base, nbase, offsets, bitmap, seg_count);
 }
@@ -1317,6 +1513,34 @@ void launch_sweep64(int L, int rpt, uint32_t nitems, const Bucket* buckets, cons
     else { if (rpt == 2) WL_S64(4, 2); else WL_S64(4, 1); }
 #undef WL_S64
 }
+void launch_acc_init(uint32_t nrows, uint32_t nbuckets, uint4* acc, Deficit* bdef, cudaStream_t st) {
+    const uint32_t n = nrows > nbuckets ? nrows : nbuckets;
+    if (!n) return;
+    k_acc_init<<<(n + 255) / 256, 256, 0, st>>>(nrows, nbuckets, acc, bdef);
+}
+void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
+                      const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef,
+                      cudaStream_t st) {
+    if (!nrows) return;
+    if (L == 2) k_merge_cta<2><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
+    else if (L == 3) k_merge_cta<3><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
+    else k_merge_cta<4><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
+}
+void launch_sweep_bits(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                       const RowMod* mods, const uint32_t* bitmap, uint64_t lo, const uint64_t* keys, uint4* part,
+                       Deficit* defs, cudaStream_t st) {
+    if (!nitems) return;
+#define WL_SB(LL, RR) k_sweep_bits<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, bitmap, lo, keys, part, defs)
+    if (L == 2) { if (rpt == 2) WL_SB(2, 2); else WL_SB(2, 1); }
+    else if (L == 3) { if (rpt == 2) WL_SB(3, 2); else WL_SB(3, 1); }
+    else { if (rpt == 2) WL_SB(4, 2); else WL_SB(4, 1); }
+#undef WL_SB
+}
+void launch_count_bits(const uint32_t* bitmap, uint64_t lo, uint64_t nwords, uint64_t key, unsigned long long* out,
+                       cudaStream_t st) {
+    if (!nwords) return;
+    k_count_bits<<<1184, 256, 0, st>>>(bitmap, lo, nwords, key, out);
+}
 void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
                   const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st) {
     if (!nrows) return;
@@ -1327,12 +1551,13 @@ void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMo
 }
 void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
                    const Deficit* defs, uint64_t K, const uint4* ipart, uint32_t row_begin,
-                   uint32_t nrows, int full, RowOut* out, cudaStream_t st, const uint4* bacc, const Deficit* bdef) {
+                   uint32_t nrows, int full, RowOut* out, cudaStream_t st, const uint4* acc1, const Deficit* def1,
+                   const uint4* acc2, const Deficit* def2) {
     if (!nrows) return;
     const unsigned g = (nrows + 127) / 128;
-    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
-    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
-    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, bacc, bdef);
+    if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
+    else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
+    else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
 }
 
 }  // namespace wl

@@ -105,6 +105,7 @@ typedef struct {
     double ms_iterate;          /* consecutive-integer tail */
     double ms_finish;           /* combine + lift */
     uint64_t h2d_bytes, d2h_bytes;
+    double ms_big;              /* columns above 2^32 (window sieve + sweep + merge), own stream */
 } wl_stats;
 
 /* Open a context on CUDA device `device`. */

@@ -962,12 +962,13 @@ constexpr uint32_t OFF_NONE = 0xFFFFFFFFu;   // prime does not reach this CTA's 
 
 __global__ void __launch_bounds__(BIG_THREADS)
 k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_t* __restrict__ base, uint32_t nbase,
-            uint32_t* __restrict__ offs, uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
+            uint32_t ncoop, uint32_t* __restrict__ offs, uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
     extern __shared__ uint32_t smem[];
     uint32_t* bm = smem;                  // BIG_WORDS words
     uint32_t* tab = smem + BIG_WORDS;     // PRE_TABLE masks
     __shared__ uint32_t wsum[BIG_THREADS / 32];
     __shared__ uint32_t sres[BIG_PRESIEVE], sinc[BIG_PRESIEVE];
+    __shared__ uint32_t s_coop[2][160];
     if (threadIdx.x < BIG_PRESIEVE) sinc[threadIdx.x] = (64u * blockDim.x) % c_pre[threadIdx.x];
     for (uint32_t i = threadIdx.x; i < PRE_TABLE; i += blockDim.x) {
         uint32_t j = 0;
@@ -989,8 +990,10 @@ k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_
         if (!(m & 1)) m += p;
         const uint64_t o = (m - cta_lo - 1) / 2;       // number = cta_lo + 2o + 1
         off[k] = o < range_bits ? (uint32_t)o : OFF_NONE;
+        if (k < ncoop) s_coop[0][k] = off[k];
     }
     __syncthreads();
+    uint32_t cur = 0;
     for (uint32_t j = 0; j < spc; ++j) {
         const uint32_t seg = seg0 + j;
         if (seg >= nseg) break;                          // uniform across the CTA
@@ -1016,7 +1019,19 @@ k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_
             bm[w] = word;
         }
         __syncthreads();
-        for (uint32_t k = threadIdx.x; k < nbase; k += blockDim.x) {
+        // primes below 1024: all threads stride over one prime's multiples; the
+        // offsets live in shared memory, read from one half and the next
+        // segment's written to the other
+        for (uint32_t k = 0; k < ncoop; ++k) {
+            const uint32_t o = s_coop[cur][k];
+            if (o == OFF_NONE) continue;
+            const uint32_t p = base[k];
+            for (uint32_t i = o + threadIdx.x * p; i < BIG_BITS; i += blockDim.x * p)
+                atomicOr(&bm[i >> 5], 1u << (i & 31));
+            if (threadIdx.x == 0) s_coop[cur ^ 1][k] = o + ((BIG_BITS - 1 - o) / p + 1) * p - BIG_BITS;
+        }
+        // larger primes: one per thread, offsets carried to the next segment
+        for (uint32_t k = ncoop + threadIdx.x; k < nbase; k += blockDim.x) {
             uint32_t o = off[k];
             if (o == OFF_NONE) continue;
             const uint32_t p = base[k];
@@ -1046,6 +1061,7 @@ k_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, const uint32_
             seg_count[seg] = t;
         }
         __syncthreads();
+        cur ^= 1;
     }
 }
 
@@ -1492,7 +1508,13 @@ void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t spc, con
     const size_t smem = (BIG_WORDS + PRE_TABLE) * sizeof(uint32_t);
     cudaFuncSetAttribute(k_sieve_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const uint32_t ncta = (nseg + spc - 1) / spc;
-    k_sieve_big<<<ncta, BIG_THREADS, smem, st>>>(lo, hi, nseg, spc, base, nbase, offsets, bitmap, seg_count);
+    // sieving primes below 1024 (base starts at 67) are marked cooperatively
+    uint32_t ncoop = 0;
+    {
+        static const uint32_t below1024 = 154;   // odd primes 67 .. 1021
+        ncoop = nbase < below1024 ? nbase : below1024;
+    }
+    k_sieve_big<<<ncta, BIG_THREADS, smem, st>>>(lo, hi, nseg, spc, base, nbase, ncoop, offsets, bitmap, seg_count);
 }
 void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,
                         cudaStream_t st) {

@@ -56,17 +56,24 @@ def batched_ranges(seed: int = 0, n: int = 256):
     return out
 
 
-def workload(name: str, rank: int, world: int, width: int = PLAIN_SMALL[1]):
-    """(ranges, q_cap, description) for this rank."""
+def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1):
+    """(ranges, q_cap, description) for this rank; width/qcap override the
+    configuration (for profiling small cases only)."""
     if name == "plain-small":
-        a = PLAIN_SMALL[0] + rank * width
-        return [(a, a + width)], 0, f"plain-small: every prime in [{a}, {a + width}), full search"
+        w = width or PLAIN_SMALL[1]
+        q = 0 if qcap < 0 else qcap
+        a = PLAIN_SMALL[0] + rank * w
+        return [(a, a + w)], q, f"plain-small: every prime in [{a}, {a + w}), " + ("full search" if not q else f"columns q < {q}")
     if name == "plain-mid":
-        a = 10**13 + rank * 10**7
-        return [(a, a + 10**7)], 2**32, f"plain-mid: every prime in [{a}, {a + 10**7}), columns q < 2^32"
+        w = width or 10**7
+        q = 2**32 if qcap < 0 else qcap
+        a = 10**13 + rank * w
+        return [(a, a + w)], q, f"plain-mid: every prime in [{a}, {a + w}), columns q < {q}"
     if name == "plain-top":
-        b = 2**62 - 1 - rank * 10**7
-        return [(b - 10**7, b)], 2**32, f"plain-top: every prime in [{b - 10**7}, {b}), columns q < 2^32"
+        w = width or 10**7
+        q = 2**32 if qcap < 0 else qcap
+        b = 2**62 - 1 - rank * w
+        return [(b - w, b)], q, f"plain-top: every prime in [{b - w}, {b}), columns q < {q}"
     if name == "batched":
         rs = batched_ranges(0)
         mine = rs[rank::world]
@@ -155,7 +162,7 @@ def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    ranges, q_cap, desc = workload(args.workload, 0, 1, args.width)
+    ranges, q_cap, desc = workload(args.workload, 0, 1, args.width, args.qcap)
     lo, hi = ranges[0]
     import oracle
     oracle.build()
@@ -193,8 +200,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain-small", choices=["plain-small", "plain-mid", "plain-top", "batched"])
-    ap.add_argument("--width", type=int, default=PLAIN_SMALL[1],
-                    help="plain-small range width per GPU (default 1e6; smaller only for profiling)")
+    ap.add_argument("--width", type=int, default=0,
+                    help="range width per GPU (default: the configuration's; smaller only for profiling)")
+    ap.add_argument("--qcap", type=int, default=-1,
+                    help="column cap q < QCAP (default: the configuration's; only for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -217,7 +226,7 @@ def main():
     import clwilson_b200 as wl
     eng = wl.Engine(local)
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
-    ranges, q_cap, desc = workload(args.workload, rank, world, args.width)
+    ranges, q_cap, desc = workload(args.workload, rank, world, args.width, args.qcap)
     L = max(limbs_for(b - 1) for a, b in ranges)
     peak_mad = wl.probe("mad", local)
     peak_cell = wl.probe("cell%d" % L, local)
@@ -225,8 +234,8 @@ def main():
 
     def step():
         eng.drop_columns()
-        if len(ranges) == 1 and q_cap == 0:
-            r = eng.search(ranges[0][0], ranges[0][1])
+        if len(ranges) == 1:
+            r = eng.search(ranges[0][0], ranges[0][1], q_cap=q_cap)
             return r.stats
         per, res, st = eng.batch(ranges, q_cap=q_cap)
         return st

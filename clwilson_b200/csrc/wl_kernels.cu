@@ -432,14 +432,15 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
 // ===========================================================================
 
 constexpr int DENSE_CHUNK = 1024;    // staged columns per CTA and pass
-constexpr int DW = 4;                // window width in bits
-constexpr int NBK = (1 << DW) - 1;   // buckets per window
 
-template <int L>
-__device__ __forceinline__ void bucket_cell(Res<L> (&B)[NBK], uint32_t d, uint32_t q, const uint32_t* n,
-                                            uint32_t ninv) {
+// cell on bucket d (1 .. NB) of a window; d is the same for every thread of a
+// split group, so the switch is a uniform branch
+template <int L, int NB>
+__device__ __forceinline__ void bucket_cell(Res<L> (&B)[NB], uint32_t d, uint32_t q, const uint32_t* n,
+                                            uint32_t ninv, bool wide) {
     switch (d) {
-#define WL_BC(k) case k: cell_w<L>(B[k - 1], q, n, ninv); break;
+#define WL_BC(k) case k: if (k <= NB) { cell_w<L>(B[(k <= NB ? k : 1) - 1], q, n, ninv); \
+                                        if (wide) cond_sub_chain(B[(k <= NB ? k : 1) - 1], n); } break;
         WL_BC(1) WL_BC(2) WL_BC(3) WL_BC(4) WL_BC(5) WL_BC(6) WL_BC(7) WL_BC(8)
         WL_BC(9) WL_BC(10) WL_BC(11) WL_BC(12) WL_BC(13) WL_BC(14) WL_BC(15)
 #undef WL_BC
@@ -447,13 +448,14 @@ __device__ __forceinline__ void bucket_cell(Res<L> (&B)[NBK], uint32_t d, uint32
     }
 }
 
-template <int L, int MINB>
+template <int L, int MINB, int DW>
 __global__ void __launch_bounds__(256, MINB)
 k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
               const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, const uint32_t* __restrict__ dsplit,
               uint4* __restrict__ part, Deficit* __restrict__ defs) {
     __shared__ uint32_t sq[DENSE_CHUNK];
     __shared__ uint64_t sm[DENSE_CHUNK];
+    constexpr int NBK = (1 << DW) - 1;          // buckets per window
     __shared__ uint32_t scnt[256][NBK + 1];     // cells per bucket, per split group
     const SweepItem it = items[blockIdx.x];
     const Bucket bk = buckets[it.bucket];
@@ -573,19 +575,7 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
             for (uint32_t k = 0; k < nh; ++k) {
                 const uint32_t d = (uint32_t)sm[base + k];
                 const uint32_t q = sq[base + k];
-                if (d) {
-                    if (L == 2 || q < 0x80000000u) bucket_cell<L>(B, d, q, n, ninv);
-                    else {
-                        bucket_cell<L>(B, d, q, n, ninv);
-                        switch (d) {
-#define WL_BS(k) case k: cond_sub_chain(B[k - 1], n); break;
-                            WL_BS(1) WL_BS(2) WL_BS(3) WL_BS(4) WL_BS(5) WL_BS(6) WL_BS(7) WL_BS(8)
-                            WL_BS(9) WL_BS(10) WL_BS(11) WL_BS(12) WL_BS(13) WL_BS(14) WL_BS(15)
-#undef WL_BS
-                            default: break;
-                        }
-                    }
-                }
+                if (d) bucket_cell<L, NBK>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
             }
         }
         // R = prod_d B_d^d by running products from the top bucket down
@@ -1483,16 +1473,20 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
 void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
                         const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st) {
     if (!nitems) return;
-    static const int minb = getenv("WL_DENSE_MINB") ? atoi(getenv("WL_DENSE_MINB")) : 2;
-    if (minb == 1) {
-        if (L == 2) k_sweep_dense<2, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
-        else if (L == 3) k_sweep_dense<3, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
-        else k_sweep_dense<4, 1><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+    // window width and CTAs per SM (measured on B200): 4-bit windows at
+    // 2 CTAs/SM for 2- and 3-limb residues, 3-bit windows at 3 CTAs/SM for
+    // 4-limb ones (fewer bucket registers, more warps); WL_DENSE_CFG overrides
+    static const int env_cfg = getenv("WL_DENSE_CFG") ? atoi(getenv("WL_DENSE_CFG")) : 0;
+    const int cfg = env_cfg ? env_cfg : (L == 4 ? 33 : 42);
+#define WL_D(LL, MB, DWB) k_sweep_dense<LL, MB, DWB><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs)
+    if (cfg == 33) {
+        if (L == 2) WL_D(2, 3, 3); else if (L == 3) WL_D(3, 3, 3); else WL_D(4, 3, 3);
+    } else if (cfg == 32) {
+        if (L == 2) WL_D(2, 2, 3); else if (L == 3) WL_D(3, 2, 3); else WL_D(4, 2, 3);
     } else {
-        if (L == 2) k_sweep_dense<2, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
-        else if (L == 3) k_sweep_dense<3, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
-        else k_sweep_dense<4, 2><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs);
+        if (L == 2) WL_D(2, 2, 4); else if (L == 3) WL_D(3, 2, 4); else WL_D(4, 2, 4);
     }
+#undef WL_D
 }
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
                     uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st) {

@@ -9,6 +9,7 @@ Mirrors the reference program's surface (mfl0p/CLWilson):
                                 result lines and checksum
   * ``rows(pmin, pmax)``        per-prime residues and quotients
   * ``batch(ranges)``           many ranges in one device pass
+  * ``Server``                  resident serving session with continuous batching
   * ``write_results(...)``      results.txt in the reference's byte format
                                 (cl_wilson.cpp:657-688, 1093-1143)
   * ``parse_uint64``            the CLI number parser (putil.c:34-116)
@@ -69,13 +70,37 @@ class _Stats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double)]
 
 
+class _ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("pad", ctypes.c_uint32), ("pool_bytes", ctypes.c_uint64),
+                ("step_cells", ctypes.c_uint64)]
+
+
+class _RequestInfo(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("state", ctypes.c_int32), ("rc", ctypes.c_int32),
+                ("tested", ctypes.c_uint64), ("checksum", ctypes.c_uint64), ("targets", ctypes.c_uint64 * 3),
+                ("cells", ctypes.c_uint64), ("results", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+                ("ms_queued", ctypes.c_double), ("ms_latency", ctypes.c_double)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint64), ("admitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("cancelled", ctypes.c_uint64), ("rows_done", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("ms_steps", ctypes.c_double),
+                ("ms_admit", ctypes.c_double), ("peak_rows", ctypes.c_uint32), ("peak_active", ctypes.c_uint32)]
+
+
+REQ_STATES = {0: "queued", 1: "active", 2: "done", 3: "cancelled", 4: "failed"}
+SERVER_ROW_BYTES = 160
+
 ROW_DTYPE = np.dtype([("p", "<u8"), ("s0", "<u8"), ("s1", "<u8"), ("rem", "<u8"), ("quot", "<u8"),
                       ("type", "<u4"), ("status", "<u4")])
 assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
-           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe", "wl_column_product_noalloc")
+           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe", "wl_column_product_noalloc",
+           "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
+           "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
 PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
 
 _lib = None
@@ -115,6 +140,20 @@ def load_library(path: str = LIB_PATH):
     L.wl_probe.restype = ctypes.c_int
     L.wl_column_product_noalloc.argtypes = [vp, ctypes.c_uint32, u64, u64, vp, ctypes.c_uint32, vp, vp]
     L.wl_column_product_noalloc.restype = ctypes.c_int
+    L.wl_server_open.argtypes = [ctypes.POINTER(_ServerOpts), ctypes.POINTER(vp)]
+    L.wl_server_submit.argtypes = [vp, u64, u64, u64, ctypes.POINTER(u64)]
+    L.wl_server_poll.argtypes = [vp, u64, ctypes.POINTER(_RequestInfo)]
+    L.wl_server_wait.argtypes = [vp, u64, ctypes.POINTER(_RequestInfo), ctypes.c_double]
+    L.wl_server_results.argtypes = [vp, u64, ctypes.POINTER(_Result), sz, ctypes.POINTER(sz)]
+    L.wl_server_rows.argtypes = [vp, u64, vp, sz, ctypes.POINTER(sz)]
+    L.wl_server_cancel.argtypes = [vp, u64]
+    L.wl_server_release.argtypes = [vp, u64]
+    L.wl_server_stats_get.argtypes = [vp, ctypes.POINTER(_ServerStats)]
+    for fn in ("wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
+               "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get"):
+        getattr(L, fn).restype = ctypes.c_int
+    L.wl_server_close.argtypes = [vp]
+    L.wl_server_close.restype = None
     _lib = L
     return L
 
@@ -266,3 +305,114 @@ class Engine:
                           status=o.status) for o in out]
         results = [(res[i].p, res[i].value) for i in range(min(nres.value, cap))]
         return per_range, results, Stats.from_c(st)
+
+
+@dataclass
+class RequestInfo:
+    id: int
+    state: str
+    rc: int
+    tested: int
+    checksum: int
+    targets: Tuple[int, int, int]
+    cells: int
+    results: int
+    ms_queued: float
+    ms_latency: float
+
+    @classmethod
+    def from_c(cls, r: _RequestInfo) -> "RequestInfo":
+        return cls(r.id, REQ_STATES.get(r.state, str(r.state)), r.rc, r.tested, r.checksum, tuple(r.targets),
+                   r.cells, r.results, r.ms_queued, r.ms_latency)
+
+
+class Server:
+    """Resident serving session (wl_server_*): ranges submitted at any time
+    are admitted into a device row pool as it frees up and share the GPU's
+    column sweeps with the requests already running; each request's results
+    equal those of ``Engine.search`` / ``Engine.rows`` on its range."""
+
+    def __init__(self, device: int = 0, pool_bytes: int = 0, step_cells: int = 0):
+        self._L = load_library()
+        self._srv = ctypes.c_void_p()
+        o = _ServerOpts(device, 0, pool_bytes, step_cells)
+        rc = self._L.wl_server_open(ctypes.byref(o), ctypes.byref(self._srv))
+        if rc:
+            raise WilsonError(rc, "wl_server_open")
+
+    def close(self) -> None:
+        if self._srv:
+            self._L.wl_server_close(self._srv)
+            self._srv = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, pmin: int, pmax: int, q_cap: int = 0) -> int:
+        rid = ctypes.c_uint64(0)
+        rc = self._L.wl_server_submit(self._srv, pmin, pmax, q_cap, ctypes.byref(rid))
+        if rc:
+            raise WilsonError(rc, "wl_server_submit")
+        return rid.value
+
+    def poll(self, rid: int) -> RequestInfo:
+        info = _RequestInfo()
+        rc = self._L.wl_server_poll(self._srv, rid, ctypes.byref(info))
+        if rc < 0:
+            raise WilsonError(rc, "wl_server_poll")
+        return RequestInfo.from_c(info)
+
+    def wait(self, rid: int, timeout_ms: float = -1.0) -> RequestInfo:
+        info = _RequestInfo()
+        rc = self._L.wl_server_wait(self._srv, rid, ctypes.byref(info), timeout_ms)
+        if rc < 0:
+            raise WilsonError(rc, "wl_server_wait")
+        return RequestInfo.from_c(info)
+
+    def results(self, rid: int) -> List[Tuple[int, int]]:
+        n = ctypes.c_size_t(0)
+        rc = self._L.wl_server_results(self._srv, rid, None, 0, ctypes.byref(n))
+        if rc:
+            raise WilsonError(rc, "wl_server_results")
+        res = (_Result * max(n.value, 1))()
+        rc = self._L.wl_server_results(self._srv, rid, res, n.value, ctypes.byref(n))
+        if rc:
+            raise WilsonError(rc, "wl_server_results")
+        return [(res[i].p, res[i].value) for i in range(n.value)]
+
+    def rows(self, rid: int) -> np.ndarray:
+        n = ctypes.c_size_t(0)
+        rc = self._L.wl_server_rows(self._srv, rid, None, 0, ctypes.byref(n))
+        if rc:
+            raise WilsonError(rc, "wl_server_rows")
+        buf = np.zeros(max(n.value, 1), dtype=ROW_DTYPE)
+        rc = self._L.wl_server_rows(self._srv, rid, buf.ctypes.data, n.value, ctypes.byref(n))
+        if rc:
+            raise WilsonError(rc, "wl_server_rows")
+        return buf[: n.value]
+
+    def cancel(self, rid: int) -> None:
+        rc = self._L.wl_server_cancel(self._srv, rid)
+        if rc:
+            raise WilsonError(rc, "wl_server_cancel")
+
+    def release(self, rid: int) -> None:
+        rc = self._L.wl_server_release(self._srv, rid)
+        if rc:
+            raise WilsonError(rc, "wl_server_release")
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        rc = self._L.wl_server_stats_get(self._srv, ctypes.byref(st))
+        if rc:
+            raise WilsonError(rc, "wl_server_stats_get")
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}

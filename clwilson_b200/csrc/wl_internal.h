@@ -37,7 +37,8 @@ struct Bucket {
                          // nearly every column), [cdense, ncols) the prefix-fold sweep
     uint32_t ndense;     // splits 0 .. ndense-1 cover the dense columns, the rest the others
     uint32_t dstart;     // dense split s covers columns [dsplit[dstart+s], dsplit[dstart+s+1])
-    uint32_t pad2;
+    uint32_t cbase;      // column offset: split ranges are relative to cols + cbase (a serving
+                         // step sweeps the chunk [cbase, cbase + ncols) of the bucket's columns)
 };
 
 // Column range [c0, c1) of split s of a bucket.  Dense splits have explicit
@@ -57,6 +58,8 @@ __host__ __device__ inline void split_range(const Bucket& b, uint32_t s, uint64_
         *c0 = b.cdense + n * j / k;
         *c1 = b.cdense + n * (j + 1) / k;
     }
+    *c0 += b.cbase;
+    *c1 += b.cbase;
 }
 
 // One CTA of the column sweep: threads [k*tps, (k+1)*tps) work on split
@@ -124,6 +127,8 @@ void launch_count_bits(const uint32_t* bitmap, uint64_t lo, uint64_t nwords, uin
 void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
                   const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_acc_init(uint32_t nrows, uint32_t nbuckets, uint4* acc, Deficit* bdef, cudaStream_t st);
+void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* ipart,
+                       uint64_t K, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,
                       const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef,
                       cudaStream_t st);

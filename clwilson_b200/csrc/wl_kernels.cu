@@ -1311,7 +1311,9 @@ k_merge(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, co
     const uint32_t row = row_begin + i;
     const uint32_t b = info[row].bucket;
     const Bucket bk = buckets[b];
-    if (bk.nsplit == 0) return;
+    // buckets without splits in this launch, other limb widths, and rows that
+    // are not (or no longer) in the bucket's row range are left alone
+    if (bk.nsplit == 0 || bk.L != (uint32_t)L || row - bk.row_begin >= bk.nrows) return;
     const RowMod m = mods[row];
     uint32_t n[L];
 #pragma unroll
@@ -1368,7 +1370,7 @@ k_merge_cta(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info
     const uint32_t row = row_begin + blockIdx.x;
     const uint32_t b = info[row].bucket;
     const Bucket bk = buckets[b];
-    if (bk.nsplit == 0) return;                      // uniform across the CTA
+    if (bk.nsplit == 0 || bk.L != (uint32_t)L || row - bk.row_begin >= bk.nrows) return;   // uniform across the CTA
     const RowMod m = mods[row];
     uint32_t n[L];
 #pragma unroll
@@ -1419,6 +1421,63 @@ k_merge_cta(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info
             bdef[b].lo = (uint64_t)tot;
             bdef[b].hi = (uint64_t)(tot >> 64);
         }
+    }
+}
+
+// Serving sessions: fold each row's consecutive-integer tail (k_iterate items
+// ipart[it_begin .. it_begin + it_count)) into its resident accumulator when
+// the row is admitted.  The tail's power of two differs per row, so it is
+// restored here; the one Montgomery product into acc removes 2^(32L) from
+// every row alike, which the bucket's first row adds to bdef[bucket].
+template <int L>
+__global__ void __launch_bounds__(128)
+k_tail_merge(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, const RowMod* __restrict__ mods,
+             const uint4* __restrict__ ipart, uint64_t K, uint32_t row_begin, uint32_t nrows,
+             uint4* __restrict__ acc, Deficit* __restrict__ bdef) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const uint32_t row = row_begin + i;
+    const RowInfo ri = info[row];
+    const Bucket bk = buckets[ri.bucket];
+    if (bk.L != (uint32_t)L || row - bk.row_begin >= bk.nrows) return;
+    const RowMod m = mods[row];
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = m.n[k];
+    Res<L> X;
+    set_small<L>(X, 1);
+    u128 def = 0;
+    for (uint32_t k = 0; k < ri.it_count; ++k) {
+        const uint4 v = ipart[ri.it_begin + k];
+        Res<L> y;
+        y.w[0] = v.x; y.w[1] = v.y;
+        if (L > 2) y.w[2 < L ? 2 : 0] = v.z;
+        if (L > 3) y.w[3 < L ? 3 : 0] = v.w;
+        X = mont_mul<L>(X, y, n, m.ninv);
+        const uint64_t start = bk.T + 1 + (uint64_t)k * K;
+        const uint64_t rest = ri.Tp - bk.T - (uint64_t)k * K;
+        const uint64_t len = rest < K ? rest : K;
+        def += (u128)len * (start + len - 1 < 0x80000000ull ? 32 : 64) + 32 * L;
+    }
+    // X * 2^def: Mont(2^def) = (2R)^def in the Montgomery domain
+    Res<L> one;
+    set_small<L>(one, 1);
+    for (int k = 0; k < 32 * L; ++k) dbl_mod<L>(one, n);
+    Res<L> two = one;
+    dbl_mod<L>(two, n);
+    X = mont_mul<L>(X, mont_pow<L>(two, def, one, n, m.ninv), n, m.ninv);
+    const uint4 a = acc[row];
+    Res<L> A;
+    A.w[0] = a.x; A.w[1] = a.y;
+    if (L > 2) A.w[2 < L ? 2 : 0] = a.z;
+    if (L > 3) A.w[3 < L ? 3 : 0] = a.w;
+    A = mont_mul<L>(A, X, n, m.ninv);
+    acc[row] = make_uint4(A.w[0], A.w[1], L > 2 ? A.w[2 < L ? 2 : 0] : 0, L > 3 ? A.w[3 < L ? 3 : 0] : 0);
+    if (row == bk.row_begin) {
+        u128 d = ((u128)bdef[ri.bucket].hi << 64) | bdef[ri.bucket].lo;
+        d += 32 * L;
+        bdef[ri.bucket].lo = (uint64_t)d;
+        bdef[ri.bucket].hi = (uint64_t)(d >> 64);
     }
 }
 
@@ -1541,6 +1600,15 @@ void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const R
     if (L == 2) k_merge_cta<2><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
     else if (L == 3) k_merge_cta<3><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
     else k_merge_cta<4><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
+}
+
+void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* ipart,
+                       uint64_t K, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st) {
+    if (!nrows) return;
+    const unsigned g = (nrows + 127) / 128;
+    if (L == 2) k_tail_merge<2><<<g, 128, 0, st>>>(buckets, info, mods, ipart, K, row_begin, nrows, acc, bdef);
+    else if (L == 3) k_tail_merge<3><<<g, 128, 0, st>>>(buckets, info, mods, ipart, K, row_begin, nrows, acc, bdef);
+    else k_tail_merge<4><<<g, 128, 0, st>>>(buckets, info, mods, ipart, K, row_begin, nrows, acc, bdef);
 }
 void launch_sweep_bits(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                        const RowMod* mods, const uint32_t* bitmap, uint64_t lo, const uint64_t* keys, uint4* part,

@@ -64,6 +64,8 @@ __global__ void k_noalloc_prep(const uint64_t* __restrict__ primes, uint32_t nro
         b.range = 0;
         b.cdense = 0;
         b.ndense = 0;
+        b.dstart = 0;
+        b.cbase = 0;
         *bk = b;
     }
     if (i < nitems) {

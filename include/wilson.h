@@ -24,6 +24,8 @@
  *                         the per-prime quotient of processResult (691-900)
  *   wl_batch              many ranges in one device pass (no counterpart: the
  *                         reference runs one range per process)
+ *   wl_server_*           a resident serving session with continuous batching
+ *                         (no counterpart: the reference is one range per process)
  *   wl_drop_columns       makes the next search sieve its columns again, as the
  *                         reference does on every run (getPrimes,
  *                         cl_wilson.cpp:1368-1397)
@@ -173,6 +175,86 @@ void wl_drop_columns(wl_ctx *ctx);
 #define WL_NOALLOC_SCRATCH_BYTES (5u << 20)
 int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p_bound, uint64_t T,
                               const uint32_t *cols, uint32_t ncols, uint64_t *s0s1, void *stream);
+
+/* ---- Serving: a resident session with continuous batching ------------------
+ *
+ * No counterpart in the reference.  A server owns one GPU and a scheduler
+ * thread.  Submitted ranges wait in a FIFO queue until the row pool (a device
+ * memory budget for resident test primes: moduli, running partial products,
+ * outputs) and the bucket table have room; then they are admitted between
+ * scheduler steps.  Each step advances every admitted (range, class) bucket by
+ * one chunk of its columns -- all buckets in the same sweep launches -- and
+ * folds the chunk's products into the bucket rows' resident partial products.
+ * Requests that finish their columns are completed (class lift, quotient,
+ * result lines, checksum) and their rows freed for the next ones, so requests
+ * that arrive while others run share the GPU with them.  Each request's
+ * results are bit-identical to wl_search / wl_rows on the same range.
+ *
+ * Limits: the columns of a request stay below 2^32 (q_cap <= 2^32, or a full
+ * search whose class targets are below 2^32: p below about 8.5e9);
+ * otherwise the request fails with WL_ERR_UNSUPPORTED.  A request larger than
+ * the whole pool fails with WL_ERR_NOMEM.  All functions are thread-safe. */
+typedef struct wl_server wl_server;
+
+typedef struct {
+    int device;
+    uint32_t pad;
+    uint64_t pool_bytes;   /* device memory for resident rows (0: 1 GiB); WL_SERVER_ROW_BYTES each */
+    uint64_t step_cells;   /* column-cell budget of one scheduler step (0: 2^32) */
+} wl_server_opts;
+
+#define WL_SERVER_ROW_BYTES 160u
+
+#define WL_REQ_QUEUED    0
+#define WL_REQ_ACTIVE    1
+#define WL_REQ_DONE      2
+#define WL_REQ_CANCELLED 3
+#define WL_REQ_FAILED    4
+
+typedef struct {
+    uint64_t id;
+    int32_t state;         /* WL_REQ_* */
+    int32_t rc;            /* 0, or the WL_ERR_* code of a failed request */
+    uint64_t tested;       /* test primes (rows) */
+    uint64_t checksum;     /* full: sum(p + rem + quot); capped: sum(p + s0 + s1), mod 2^64 */
+    uint64_t targets[3];   /* class targets */
+    uint64_t cells;        /* column cells + tail steps of the request */
+    uint32_t results;      /* result lines (full searches) */
+    uint32_t pad;
+    double ms_queued;      /* submit -> admission */
+    double ms_latency;     /* submit -> completion */
+} wl_request_info;
+
+typedef struct {
+    uint64_t steps;        /* scheduler steps run */
+    uint64_t admitted, completed, failed, cancelled;
+    uint64_t rows_done;    /* rows of completed requests */
+    uint64_t cells;        /* cells of completed requests */
+    uint64_t launches;     /* kernel launches */
+    double ms_steps;       /* device time of the steps (CUDA events) */
+    double ms_admit;       /* device time of admissions */
+    uint32_t peak_rows;    /* largest number of resident rows */
+    uint32_t peak_active;  /* largest number of admitted requests at once */
+} wl_server_stats;
+
+int wl_server_open(const wl_server_opts *opts, wl_server **out);
+/* Queue [pmin, pmax) (q_cap as in wl_search); *id identifies the request. */
+int wl_server_submit(wl_server *srv, uint64_t pmin, uint64_t pmax, uint64_t q_cap, uint64_t *id);
+/* 0 if the request has ended (done, failed or cancelled), 1 if not; fills *info. */
+int wl_server_poll(wl_server *srv, uint64_t id, wl_request_info *info);
+/* As poll, waiting up to timeout_ms (< 0: no limit) for the request to end. */
+int wl_server_wait(wl_server *srv, uint64_t id, wl_request_info *info, double timeout_ms);
+/* Result lines of a finished full search, ascending p (WL_ERR_CAPACITY if cap is short). */
+int wl_server_results(wl_server *srv, uint64_t id, wl_result *results, size_t cap, size_t *n);
+/* Rows of a finished request, ascending p, as wl_rows. */
+int wl_server_rows(wl_server *srv, uint64_t id, wl_row *rows, size_t cap, size_t *n);
+/* Cancel a queued or running request; it ends in WL_REQ_CANCELLED. */
+int wl_server_cancel(wl_server *srv, uint64_t id);
+/* Forget an ended request (its id becomes invalid). */
+int wl_server_release(wl_server *srv, uint64_t id);
+int wl_server_stats_get(wl_server *srv, wl_server_stats *stats);
+/* Stop the scheduler (running requests are abandoned) and free the server. */
+void wl_server_close(wl_server *srv);
 
 /* parse_uint64 of the reference CLI: returns 0, -1 (cannot parse) or -2 (out of range). */
 int wl_parse_uint64(uint64_t *result, const char *str, uint64_t lo, uint64_t hi);

@@ -1,0 +1,106 @@
+"""Serving sessions (wl_server_*): continuous batching over a resident row pool.
+
+Each request's rows, result lines and checksum must be bit-identical to the
+one-shot engine (wl_search / wl_rows) on the same range, whether the request
+runs alone or shares the GPU's column sweeps with other requests, whatever
+the step size (column chunking) and however full the row pool is (queueing).
+"""
+import numpy as np
+import pytest
+
+import clwilson_b200 as wl
+
+pytestmark = pytest.mark.gpu
+
+FULL = [(200, 564), (10**6, 10**6 + 5000), (2**31 - 1000, 2**31 + 1000), (10**9, 10**9 + 20000)]
+CAPPED = [(10**13, 10**13 + 10000, 1 << 22), ((1 << 62) - 30000, (1 << 62) - 1, 1 << 22),
+          (10**9, 10**9 + 10000, 1 << 22), (10**8, 10**8 + 4000, 1 << 20)]
+
+
+@pytest.fixture(scope="module")
+def expected(engine):
+    exp = {}
+    for lo, hi in FULL:
+        r = engine.search(lo, hi)
+        rows, _ = engine.rows(lo, hi)
+        exp[(lo, hi, 0)] = (r.checksum, r.results, rows)
+    for lo, hi, q in CAPPED:
+        rows, _ = engine.rows(lo, hi, q_cap=q)
+        ck = int((rows["p"].astype(object) + rows["s0"].astype(object) + rows["s1"].astype(object)).sum()) % (1 << 64)
+        exp[(lo, hi, q)] = (ck, [], rows)
+    return exp
+
+
+def _check(srv, rid, key, expected):
+    info = srv.wait(rid, 600_000)
+    assert info.state == "done", (key, info)
+    ck, results, rows = expected[key]
+    assert info.checksum == ck, key
+    assert info.tested == len(rows)
+    got = srv.rows(rid)
+    for f in ("p", "s0", "s1", "rem", "quot", "type"):
+        assert np.array_equal(got[f], rows[f]), (key, f)
+    if key[2] == 0:
+        assert srv.results(rid) == results
+    return info
+
+
+def _all_keys():
+    return [(lo, hi, 0) for lo, hi in FULL] + list(CAPPED)
+
+
+def test_alone(expected):
+    with wl.Server(0) as srv:
+        for key in _all_keys():
+            rid = srv.submit(*key)
+            _check(srv, rid, key, expected)
+            srv.release(rid)
+
+
+@pytest.mark.parametrize("step_cells", [0, 1 << 24])
+def test_mixed(expected, step_cells):
+    # everything at once, and a second wave submitted while the first runs
+    with wl.Server(0, step_cells=step_cells) as srv:
+        keys = _all_keys()
+        ids = [srv.submit(*k) for k in keys]
+        ids2 = [srv.submit(*k) for k in reversed(keys)]
+        for rid, k in zip(ids + ids2, keys + list(reversed(keys))):
+            _check(srv, rid, k, expected)
+        st = srv.stats()
+        assert st["completed"] == 2 * len(keys) and st["failed"] == 0
+        assert st["peak_active"] > 1
+
+
+def test_small_pool_queues(expected):
+    # a pool of 2500 rows: the 1e9 full range (~980 rows) and the capped ones
+    # (~300-1500 rows) cannot all be resident; they queue and still match
+    with wl.Server(0, pool_bytes=2500 * wl.SERVER_ROW_BYTES, step_cells=1 << 26) as srv:
+        keys = _all_keys()
+        ids = [srv.submit(*k) for k in keys]
+        infos = [_check(srv, rid, k, expected) for rid, k in zip(ids, keys)]
+        assert srv.stats()["peak_rows"] <= 2500
+        assert max(i.ms_queued for i in infos) > 0
+
+
+def test_cancel_and_errors(expected):
+    with wl.Server(0, step_cells=1 << 24) as srv:
+        big = srv.submit(10**13, 10**13 + 10**6, 1 << 30)     # long-running
+        small = srv.submit(*CAPPED[0])
+        srv.cancel(big)
+        assert srv.wait(big, 600_000).state == "cancelled"
+        _check(srv, small, CAPPED[0], expected)
+        # full search with class targets above 2^32: not served
+        bad = srv.submit(10**13, 10**13 + 1000)
+        info = srv.wait(bad, 600_000)
+        assert info.state == "failed" and info.rc == -4
+        # no primes in [24, 29)
+        none = srv.submit(24, 29)
+        info = srv.wait(none, 600_000)
+        assert info.state == "failed" and info.rc == -3
+        with pytest.raises(wl.WilsonError):
+            srv.submit(10**9, 10**9 + 100, (1 << 32) + 1)
+        with pytest.raises(wl.WilsonError):
+            srv.submit(4, 100)
+        # the server keeps serving after failures
+        rid = srv.submit(*CAPPED[3])
+        _check(srv, rid, CAPPED[3], expected)

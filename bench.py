@@ -9,7 +9,17 @@ Workloads (--workload):
                 (the full run is about a day on one GPU); partial products per prime.
   plain-top     every prime in [2^62-1-1e7, 2^62-1): column sweep capped at q < 2^32.
   batched       256 ranges from numpy default_rng(0), log-uniform starts in
-                [1e8, 2^62-1e7) and widths in [1e3, 1e7], column sweep capped at q < 2^28.
+                [1e8, 2^62-1e7) and widths in [1e3, 1e7], each width truncated to
+                --max-width integers (default 2000: the whole widths are about 9e6
+                rows, 1.3e14 column cells, hours per step), column sweep capped at
+                q < 2^28.  One wl_batch call per step; the same ranges as a loop of
+                per-range wl_search calls (the plain form) are timed beside it.
+  serving       a Poisson stream of --requests range requests (default 256) from
+                numpy default_rng(1): exponential inter-arrival times at --rate
+                requests/s, log-uniform starts in [1e8, 2^62-1e7), widths
+                log-uniform in [1e4, 1e7] truncated to --max-width; q < 2^28.
+                Submitted to a serving session (wl_server_*) at their arrival
+                times; a step is the whole stream.  Reports p50/p99 latency.
 
 A step is one call of the engine's C ABI on the workload (test primes, columns,
 sweep, tail, lift, results).  `value` is device time (CUDA events on the
@@ -42,7 +52,7 @@ def limbs_for(pmax_incl: int) -> int:
     return 2 if pmax_incl < 2**31 else (3 if pmax_incl < 2**47 else 4)
 
 
-def batched_ranges(seed: int = 0, n: int = 256):
+def batched_ranges(seed: int = 0, n: int = 256, max_width: int = 0):
     import numpy as np
     rng = np.random.default_rng(seed)
     lo, hi = np.log(1e8), np.log(2.0**62 - 1e7)
@@ -51,12 +61,30 @@ def batched_ranges(seed: int = 0, n: int = 256):
     out = []
     for s, w in zip(starts, widths):
         a = int(s)
-        b = min(a + int(w), 2**62 - 1)
+        w = int(w) if not max_width else min(int(w), max_width)
+        b = min(a + w, 2**62 - 1)
         out.append((max(a, 5), b))
     return out
 
 
-def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1):
+def serving_requests(seed: int = 1, n: int = 256, rate: float = 64.0, max_width: int = 0):
+    """(arrival time in s, pmin, pmax) of a Poisson stream of range requests."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(1e8), np.log(2.0**62 - 1e7)
+    starts = np.exp(rng.uniform(lo, hi, n))
+    widths = np.round(np.exp(rng.uniform(np.log(1e4), np.log(1e7), n)))
+    gaps = rng.exponential(1.0 / rate, n)
+    t = np.cumsum(gaps) - gaps[0]
+    out = []
+    for ti, s, w in zip(t, starts, widths):
+        a = max(int(s), 5)
+        w = int(w) if not max_width else min(int(w), max_width)
+        out.append((float(ti), a, min(a + w, 2**62 - 1)))
+    return out
+
+
+def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1, max_width: int = 2000):
     """(ranges, q_cap, description) for this rank; width/qcap override the
     configuration (for profiling small cases only)."""
     if name == "plain-small":
@@ -75,9 +103,11 @@ def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1):
         b = 2**62 - 1 - rank * w
         return [(b - w, b)], q, f"plain-top: every prime in [{b - w}, {b}), columns q < {q}"
     if name == "batched":
-        rs = batched_ranges(0)
+        rs = batched_ranges(0, max_width=max_width)
         mine = rs[rank::world]
-        return mine, 2**28, f"batched: {len(mine)} of 256 ranges from default_rng(0), columns q < 2^28"
+        q = 2**28 if qcap < 0 else qcap
+        return mine, q, (f"batched: {len(mine)} of 256 ranges from default_rng(0), widths truncated to "
+                         f"{max_width}, columns q < {q}")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -193,13 +223,106 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_serving(args, rank, world, local):
+    """The serving stream: submit each request at its arrival time, wait for
+    all, report throughput over the stream and request latencies."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import clwilson_b200 as wl
+    q_cap = 2**28 if args.qcap < 0 else args.qcap
+    reqs = serving_requests(1, args.requests, args.rate, args.max_width)[rank::world]
+    L = max(limbs_for(b - 1) for _, a, b in reqs)
+    peak_mad = wl.probe("mad", local)
+    srv = wl.Server(local)
+
+    def stream(reqs, clk=None):
+        ids = []
+        t0 = time.perf_counter()
+        for t, a, b in reqs:
+            dt = t - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(a, b, q_cap))
+        infos = [srv.wait(i, 3600e3) for i in ids]
+        t1 = time.perf_counter()
+        for i in ids:
+            srv.release(i)
+        return infos, t1 - t0
+
+    # warm-up: a few requests through the session (column cache, first launches)
+    for _ in range(max(3, args.warmup)):
+        stream(reqs[:4])
+    st0 = srv.stats()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        infos, wall = stream(reqs)
+    st1 = srv.stats()
+    bad = [i for i in infos if i.state != "done"]
+    cells = sum(i.cells for i in infos)
+    rows = sum(i.tested for i in infos)
+    busy_s = ((st1["ms_steps"] - st0["ms_steps"]) + (st1["ms_admit"] - st0["ms_admit"])) / 1e3
+    lat = np.array([i.ms_latency for i in infos])
+    if dist:
+        t = torch.tensor([wall, busy_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall, busy_s = t.tolist()
+        c = torch.tensor([cells, rows], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        cells, rows = c.tolist()
+    line = {
+        "metric": "128-bit mulmods/s (capped column sweep, serving)", "value": cells / busy_s,
+        "unit": "mulmods/s", "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup),
+        "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"serving: {len(reqs)} requests from default_rng(1), Poisson at {args.rate}/s, "
+                               f"widths truncated to {args.max_width}, columns q < {q_cap}",
+                   "rate_per_s": args.rate, "requests": len(reqs), "q_cap": q_cap, "limbs_max": L,
+                   "test_primes": rows, "column_mulmods": cells,
+                   "l2": "inputs (row pool + column table) exceed L2 across the stream",
+                   "parallelism": f"requests sharded round-robin, dp{world}"},
+        "e2e": {"value": cells / wall, "unit": "mulmods/s", "primes_per_s": rows / wall,
+                "h2d_bytes_per_step": 16 * len(reqs), "d2h_bytes_per_step": 48 * int(rows)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()), "mean": float(lat.mean())},
+        "queue_ms_p50": float(np.percentile([i.ms_queued for i in infos], 50)),
+        "failed": len(bad),
+        "server": {k: st1[k] - st0[k] for k in ("steps", "admitted", "completed", "launches")} |
+                  {"peak_active": st1["peak_active"], "busy_s": busy_s},
+        "gpu_launches": st1["launches"] - st0["launches"],
+        "roofline": {"bound": "imad", "peak": peak_mad / 1e12, "unit": "TOP/s", "achieved": None, "frac": None,
+                     "traffic": None, "note": "device-busy throughput; see the batched and plain lines for the kernels",
+                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    srv.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain-small", choices=["plain-small", "plain-mid", "plain-top", "batched"])
+    ap.add_argument("--workload", default="plain-small",
+                    choices=["plain-small", "plain-mid", "plain-top", "batched", "serving"])
+    ap.add_argument("--max-width", type=int, default=2000,
+                    help="batched/serving: truncate each range to this many integers (0: whole ranges)")
+    ap.add_argument("--requests", type=int, default=256, help="serving: requests in the stream")
+    ap.add_argument("--rate", type=float, default=64.0, help="serving: mean arrival rate, requests/s")
+    ap.add_argument("--plain-steps", type=int, default=2, help="batched: timed passes of the plain per-range loop")
     ap.add_argument("--width", type=int, default=0,
                     help="range width per GPU (default: the configuration's; smaller only for profiling)")
     ap.add_argument("--qcap", type=int, default=-1,
@@ -213,6 +336,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "serving":
+        return run_serving(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -226,7 +351,7 @@ def main():
     import clwilson_b200 as wl
     eng = wl.Engine(local)
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
-    ranges, q_cap, desc = workload(args.workload, rank, world, args.width, args.qcap)
+    ranges, q_cap, desc = workload(args.workload, rank, world, args.width, args.qcap, args.max_width)
     L = max(limbs_for(b - 1) for a, b in ranges)
     peak_mad = wl.probe("mad", local)
     peak_cell = wl.probe("cell%d" % L, local)
@@ -318,8 +443,47 @@ def main():
         "phase_ms_per_step": {k: sum(getattr(s, "ms_" + k) for s in stats) / args.steps
                               for k in ("primes", "sieve", "sweep", "iterate", "finish")},
     }
+    if len(ranges) > 1 and args.plain_steps > 0:
+        # the plain form: one wl_search per range, same ranges, same column cap
+        per_b, _, _ = eng.batch(ranges, q_cap=q_cap)
+
+        def plain():
+            eng.drop_columns()
+            cks, cells_p = [], 0
+            for a, b in ranges:
+                if q_cap:
+                    rows, st = eng.rows(a, b, q_cap=q_cap)
+                    cks.append(int((rows["p"].astype(object) + rows["s0"].astype(object)
+                                    + rows["s1"].astype(object)).sum()) % (1 << 64))
+                else:
+                    r = eng.search(a, b)
+                    st = r.stats
+                    cks.append(r.checksum)
+                cells_p += st.cells
+            return cks, cells_p
+        cks, _ = plain()
+        pdev, pwall = [], []
+        for _ in range(args.plain_steps):
+            flush.add_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t0 = time.perf_counter()
+            cks, cells_p = plain()
+            t1 = time.perf_counter()
+            e1.record(stream)
+            e1.synchronize()
+            pdev.append(e0.elapsed_time(e1) / 1e3)
+            pwall.append(t1 - t0)
+        line["plain_form"] = {
+            "value": cells_p * len(pdev) / sum(pdev), "unit": line["unit"],
+            "e2e": cells_p * len(pwall) / sum(pwall), "ms_per_pass": 1e3 * sum(pdev) / len(pdev),
+            "passes": len(pdev), "calls_per_pass": len(ranges),
+            "per_range_checksums_equal": [pb["checksum"] for pb in per_b] == cks,
+        }
+        line["batched_over_plain"] = line["value"] / line["plain_form"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        lo, hi = ranges[0]
+        lo, hi = max(ranges, key=lambda r: r[1] - r[0])
         cb, _, _ = cpu_baseline(lo, hi, q_cap)
         if not full:
             cb["note"] = "capped sweep: value is primes/s of the capped partial products"

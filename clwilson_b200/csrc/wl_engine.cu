@@ -575,6 +575,51 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         groups.push_back({ L, rpt, dense, {} });
         return groups.back().items;
     };
+    // splits per bucket: dense (Sd) and sparse (Ss); `scale` < 1 lengthens all
+    // splits when the split partials (16 bytes per split and row) would not fit
+    // the partial-product budget
+    auto plan_splits = [&](size_t i, double scale, uint64_t* Sd_out, uint64_t* Ss_out) {
+        const uint32_t nrows_b = (uint32_t)hb[i].primes.size();
+        const int rpt = nrows_b >= 512 ? 2 : 1;
+        const uint64_t nd = ndn[i], ns = ncol[i] - nd;
+        uint64_t Sd = 0, Ss = 0;
+        if (nd > 0) {
+            // dense splits of equal estimated cost, 256 to 1024 columns long so
+            // that the per-split bucket combination stays small
+            Sd = (uint64_t)std::ceil(dcost[i] * target_threads / W);
+            Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
+            Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
+            Sd = std::max<uint64_t>(1, (uint64_t)((double)Sd * scale));
+        }
+        if (ns > 0) {
+            Ss = (uint64_t)std::ceil((double)rpt * (double)ns * target_threads / W);
+            // at most 2^17 columns per split: a bucket whose share of the threads
+            // is small (few rows next to much dense work) would otherwise run as a
+            // few very long CTAs that finish long after everything else
+            Ss = std::max<uint64_t>(Ss, (ns + (1u << 17) - 1) >> 17);
+            Ss = std::max<uint64_t>(1, std::min<uint64_t>(Ss, std::max<uint64_t>(1, ns / 2048)));
+            Ss = std::max<uint64_t>(1, (uint64_t)((double)Ss * scale));
+        }
+        if (Sd + Ss == 0) Ss = 1;
+        *Sd_out = Sd;
+        *Ss_out = Ss;
+    };
+    double scale = 1.0;
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); free_b = 8ull << 30; }
+        const double budget = std::min<double>((double)(free_b + c->part.cap) / 3.0, 24.0 * (1ull << 30)) / 16.0;
+        for (int it = 0; it < 8; ++it) {
+            double tot = 0;
+            for (size_t i = 0; i < nb; ++i) {
+                uint64_t a, b2;
+                plan_splits(i, scale, &a, &b2);
+                tot += (double)(a + b2) * (double)hb[i].primes.size();
+            }
+            if (tot <= budget) break;
+            scale *= 0.9 * budget / tot;
+        }
+    }
     for (uint32_t oi = 0; oi < border.size(); ++oi) {
         const uint32_t i = border[oi];
         const HostBucket& h = hb[i];
@@ -590,33 +635,33 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         if (b.nrows >= 512) { rpt = 2; tps = 256; }
         else if (b.nrows >= 256) { rpt = 1; tps = 256; }
         else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
-        const uint64_t nd = ndn[i], ns = b.ncols - nd;
+        const uint64_t nd = ndn[i];
         uint64_t Sd = 0, Ss = 0;
-        if (nd > 0) {
-            // dense splits of equal estimated cost, each worth >= 20000 cells per
-            // row so that the per-split bucket combination stays small
-            Sd = (uint64_t)std::ceil(dcost[i] * target_threads / W);
-            Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
-            Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
-        }
-        if (ns > 0) {
-            Ss = (uint64_t)std::ceil((double)rpt * (double)ns * target_threads / W);
-            Ss = std::max<uint64_t>(1, std::min<uint64_t>(Ss, std::max<uint64_t>(1, ns / 2048)));
-        }
-        if (Sd + Ss == 0) Ss = 1;
+        plan_splits(i, scale, &Sd, &Ss);
         b.cdense = (uint32_t)nd;
         b.ndense = (uint32_t)Sd;
         b.dstart = (uint32_t)dkeys_bucket_start.size();
         b.cbase = 0;
         dkeys_bucket_start.push_back((uint32_t)dkeys.size());
         dkeys_n.push_back((uint32_t)Sd);
-        // interior boundaries at equal cumulative cost (values q: split k ends at q_k)
+        // interior boundaries at equal cumulative cost (values q: split k ends at
+        // q_k), interpolated inside a grid step: there are more splits than grid
+        // points when the dense region is long, and a boundary snapped to the
+        // grid would leave empty splits next to ones many times too long
         for (uint64_t k = 1; k < Sd; ++k) {
             const std::vector<double>& cum = dcum[i];
+            const std::vector<double>& grid = dgrid[i];
             const double target = cum.back() * (double)k / (double)Sd;
             size_t j = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
             if (j >= cum.size()) j = cum.size() - 1;
-            dkeys.push_back((uint64_t)dgrid[i][j]);
+            double q = grid[j];
+            if (j > 0 && cum[j] > cum[j - 1]) {
+                // the cost per unit of ln q grows about like q inside a step:
+                // linear in q between the grid points
+                const double f = (target - cum[j - 1]) / (cum[j] - cum[j - 1]);
+                q = grid[j - 1] + f * (grid[j] - grid[j - 1]);
+            }
+            dkeys.push_back((uint64_t)q);
         }
         b.nsplit = (uint32_t)(Sd + Ss);
         const uint64_t S = b.nsplit;

@@ -682,13 +682,16 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             }
         }
         if (Sd) {
-            auto& items = group_for((int)b.L, 1, true);
-            if (tps == 256) {
-                for (uint32_t r0 = 0; r0 < b.nrows; r0 += 256)
+            int drpt;
+            uint32_t dtps;
+            dense_shape(b.nrows, &drpt, &dtps);
+            auto& items = group_for((int)b.L, drpt, true);
+            if (dtps == 256) {
+                for (uint32_t r0 = 0; r0 < b.nrows; r0 += 256 * drpt)
                     for (uint32_t s2 = 0; s2 < Sd; ++s2) items.push_back({ oi, r0, s2, 256u });
             } else {
-                const uint32_t per = 256 / tps;
-                for (uint32_t s2 = 0; s2 < Sd; s2 += per) items.push_back({ oi, 0, s2, (uint32_t)tps });
+                const uint32_t per = 256 / dtps;
+                for (uint32_t s2 = 0; s2 < Sd; s2 += per) items.push_back({ oi, 0, s2, dtps });
             }
         }
         for (uint32_t k = 0; k < b.nrows; ++k) {
@@ -796,7 +799,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             forked = true;
         }
         if (g.dense)
-            launch_sweep_dense(g.L, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
+            launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint32_t>(c->dsplit),
                                as<uint4>(c->part), as<Deficit>(c->defs), c->st2);
         else
@@ -1490,11 +1493,16 @@ static int serve_step(wl_server* s) {
         x = s->pdesc[w.bid];
         x.cbase = (uint32_t)w.c0;
         x.ncols = (uint32_t)w.len;
-        int rpt = 1, tps = 256;
-        if (!w.dense && b.nrows >= 512) rpt = 2;
-        if (b.nrows < 256) { tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
+        int rpt = 1;
+        uint32_t tps = 256;
+        if (w.dense) {
+            dense_shape(b.nrows, &rpt, &tps);
+        } else {
+            if (b.nrows >= 512) rpt = 2;
+            if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
+        }
         const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
-        uint64_t S = (uint64_t)std::ceil((w.dense ? 1.0 : (double)rpt) * per / (double)b.nrows * (double)w.len *
+        uint64_t S = (uint64_t)std::ceil((double)rpt * per / (double)b.nrows * (double)w.len *
                                          target_threads / W);
         const uint64_t minlen = w.dense ? 256 : 2048;
         S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, w.len / minlen)));
@@ -1510,18 +1518,18 @@ static int serve_step(wl_server* s) {
         bucket_splits[w.bid] = (uint32_t)S;
         Grp* g = nullptr;
         for (auto& gg : groups)
-            if (gg.L == (int)b.L && gg.rpt == (w.dense ? 1 : rpt) && gg.dense == w.dense) g = &gg;
+            if (gg.L == (int)b.L && gg.rpt == rpt && gg.dense == w.dense) g = &gg;
         if (!g) {
-            groups.push_back({ (int)b.L, w.dense ? 1 : rpt, w.dense, {} });
+            groups.push_back({ (int)b.L, rpt, w.dense, {} });
             g = &groups.back();
         }
         if (tps == 256) {
-            const uint32_t tile = 256 * (w.dense ? 1 : rpt);
+            const uint32_t tile = 256 * rpt;
             for (uint32_t r = 0; r < b.nrows; r += tile)
                 for (uint32_t s2 = 0; s2 < S; ++s2) g->items.push_back({ w.bid, r, s2, 256u });
         } else {
             const uint32_t per_cta = 256 / tps;
-            for (uint32_t s2 = 0; s2 < S; s2 += per_cta) g->items.push_back({ w.bid, 0, s2, (uint32_t)tps });
+            for (uint32_t s2 = 0; s2 < S; s2 += per_cta) g->items.push_back({ w.bid, 0, s2, tps });
         }
     }
     std::vector<SweepItem> all;
@@ -1536,7 +1544,7 @@ static int serve_step(wl_server* s) {
     size_t ioff = 0;
     for (auto& g : groups) {
         if (g.dense)
-            launch_sweep_dense(g.L, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
+            launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(c->part),
                                as<Deficit>(c->defs), c->st);
         else

@@ -1,6 +1,7 @@
 // wl_internal.h -- data layout shared by the CUDA kernels and the host engine.
 #pragma once
 #include <stdint.h>
+#include <stdlib.h>
 #include <cuda_runtime.h>
 
 namespace wl {
@@ -62,6 +63,21 @@ __host__ __device__ inline void split_range(const Bucket& b, uint32_t s, uint64_
     *c1 += b.cbase;
 }
 
+// Shape of the dense sweep for a bucket of nrows rows: rows per thread (1; 2
+// with WL_DENSE_RPT=2) and threads per split (256, or the power of two >= 8
+// that covers the rows of a small bucket).
+inline void dense_shape(uint32_t nrows, int* rpt, uint32_t* tps) {
+    static const int env_rpt = getenv("WL_DENSE_RPT") ? atoi(getenv("WL_DENSE_RPT")) : 0;
+    const int r = (env_rpt == 2 && nrows >= 64) ? 2 : 1;
+    uint32_t t = 256;
+    if (nrows < 256u * (uint32_t)r) {
+        t = 8;   // at most 32 splits per CTA
+        while (t * (uint32_t)r < nrows) t <<= 1;
+    }
+    *rpt = r;
+    *tps = t;
+}
+
 // One CTA of the column sweep: threads [k*tps, (k+1)*tps) work on split
 // split0 + k; thread i of a group takes rows row0 + i + j*tps, j < RPT.
 struct SweepItem {
@@ -109,8 +125,9 @@ void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
-void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
-                        const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st);
+void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                        const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
+                        cudaStream_t st);
 void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t segs_per_cta, const uint32_t* base,
                       uint32_t nbase, uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
 void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,

@@ -433,14 +433,19 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
 
 constexpr int DENSE_CHUNK = 1024;    // staged columns per CTA and pass
 
-// cell on bucket d (1 .. NB) of a window; d is the same for every thread of a
-// split group, so the switch is a uniform branch
-template <int L, int NB>
-__device__ __forceinline__ void bucket_cell(Res<L> (&B)[NB], uint32_t d, uint32_t q, const uint32_t* n,
-                                            uint32_t ninv, bool wide) {
+// cell on bucket d (1 .. NB) of a window for each of the thread's RPT rows; d
+// is the same for every thread of a split group (the rows of a bucket share
+// their exponents), so the switch is a uniform branch and the RPT cells of a
+// case are independent chains the compiler interleaves
+template <int L, int NB, int RPT>
+__device__ __forceinline__ void bucket_cell(Res<L> (&B)[RPT][NB], uint32_t d, uint32_t q,
+                                            const uint32_t (&n)[RPT][L], const uint32_t (&ninv)[RPT], bool wide) {
     switch (d) {
-#define WL_BC(k) case k: if (k <= NB) { cell_w<L>(B[(k <= NB ? k : 1) - 1], q, n, ninv); \
-                                        if (wide) cond_sub_chain(B[(k <= NB ? k : 1) - 1], n); } break;
+#define WL_BC(k) case k: if (k <= NB) {                                                   \
+            _Pragma("unroll") for (int j = 0; j < RPT; ++j) {                             \
+                cell_w<L>(B[j][(k <= NB ? k : 1) - 1], q, n[j], ninv[j]);                 \
+                if (wide) cond_sub_chain(B[j][(k <= NB ? k : 1) - 1], n[j]);              \
+            } } break;
         WL_BC(1) WL_BC(2) WL_BC(3) WL_BC(4) WL_BC(5) WL_BC(6) WL_BC(7) WL_BC(8)
         WL_BC(9) WL_BC(10) WL_BC(11) WL_BC(12) WL_BC(13) WL_BC(14) WL_BC(15)
 #undef WL_BC
@@ -448,34 +453,50 @@ __device__ __forceinline__ void bucket_cell(Res<L> (&B)[NB], uint32_t d, uint32_
     }
 }
 
-template <int L, int MINB, int DW>
+// One CTA: 256/tps splits of one bucket (groups of tps threads, tps >= 8);
+// thread lt of a group takes rows row0 + lt + j*tps, j < RPT.  H changes about
+// once per `hstep` columns of a split.
+//
+// SORT = 1: each staged chunk of a window pass is counting-sorted by digit in
+// shared memory, and the cells of digit d run as a straight loop into bucket d
+// (no per-column branch), alternating between the bucket and a second chain X
+// that is folded into the bucket at the end of the digit's run (one Montgomery
+// product when the run has two or more columns).
+constexpr uint32_t DENSE_GMAX = 32;   // splits per CTA at most (tps >= 8)
+
+template <int L, int MINB, int DW, int RPT, int SORT>
 __global__ void __launch_bounds__(256, MINB)
 k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
               const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, const uint32_t* __restrict__ dsplit,
-              uint4* __restrict__ part, Deficit* __restrict__ defs) {
+              uint4* __restrict__ part, Deficit* __restrict__ defs, uint32_t hstep) {
     __shared__ uint32_t sq[DENSE_CHUNK];
     __shared__ uint64_t sm[DENSE_CHUNK];
+    __shared__ uint32_t ss[SORT ? DENSE_CHUNK : 1];       // chunk sorted by digit
     constexpr int NBK = (1 << DW) - 1;          // buckets per window
-    __shared__ uint32_t scnt[256][NBK + 1];     // cells per bucket, per split group
+    __shared__ uint32_t scnt[DENSE_GMAX][NBK + 1];        // deficit of bucket d, in units of 32 bits
+    __shared__ uint32_t scur[SORT ? DENSE_GMAX : 1][NBK + 1];
     const SweepItem it = items[blockIdx.x];
     const Bucket bk = buckets[it.bucket];
     const uint32_t tps = it.tps;
     const uint32_t G = 256 / tps;                 // splits in this CTA
+    if (G > DENSE_GMAX) return;                   // per-group tables hold DENSE_GMAX (host plans tps >= 8)
     const uint32_t g = threadIdx.x / tps, lt = threadIdx.x % tps;
     const uint32_t KG = DENSE_CHUNK / G;          // staged columns per split and chunk
     const uint32_t s = it.split0 + g;
     const bool has_split = s < bk.ndense;
-    const uint32_t r = it.row0 + lt;
-    const bool live = has_split && r < bk.nrows;
     const uint64_t T = bk.T;
 
-    uint32_t n[L];
-    uint32_t ninv;
-    {
+    uint32_t n[RPT][L];
+    uint32_t ninv[RPT];
+    bool live[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        const uint32_t r = it.row0 + lt + j * tps;
+        live[j] = has_split && r < bk.nrows;
         const RowMod m = mods[bk.row_begin + (r < bk.nrows ? r : 0)];
 #pragma unroll
-        for (int k = 0; k < L; ++k) n[k] = m.n[k];
-        ninv = m.ninv;
+        for (int k = 0; k < L; ++k) n[j][k] = m.n[k];
+        ninv[j] = m.ninv;
     }
     uint64_t c0 = 0, c1 = 0;
     if (has_split) split_range(bk, s, &c0, &c1, dsplit);
@@ -489,14 +510,14 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     }
     const uint32_t nchunks = (uint32_t)((maxlen + KG - 1) / KG);
 
-    // exponent split e = H*2^sb + l: H changes about once per 64 columns
+    // exponent split e = H*2^sb + l: H changes about once per hstep columns
     uint32_t sb = 0;
     uint64_t e_first = 0;
     if (c1 > c0) {
         e_first = legendre(T, cols[c0]);
         const uint64_t e_last = legendre(T, cols[c1 - 1]);
         const uint64_t span = e_first - e_last;
-        const uint64_t per = (c1 - c0) / 64 + 1;
+        const uint64_t per = (c1 - c0) / hstep + 1;
         const uint64_t want = span / per;         // H steps wanted: span / 2^sb <= per
         while (sb < 63 && (want >> sb) != 0) ++sb;
         const uint32_t top = 64 - __clzll((long long)e_first);
@@ -507,9 +528,9 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     const uint32_t base = g * KG;
 
     // ---- pass 0: prefix product on H ----
-    Res<L> P, A;
-    set_small<L>(P, 1);
-    set_small<L>(A, 1);
+    Res<L> P[RPT], A[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) { set_small<L>(P[j], 1); set_small<L>(A[j], 1); }
     u128 defA = 0;
     uint64_t h_cur = e_first >> sb;
     uint32_t cells = 0;
@@ -529,91 +550,167 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
             const uint64_t h = sm[base + k];
             if (h != h_cur) {
                 const uint64_t d = h_cur - h;
-                fold_pow<L>(A, P, d, n, ninv);
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
                 defA += (u128)d * (32ull * cells + 32 * L);
                 h_cur = h;
             }
             const uint32_t q = sq[base + k];
-            if (L == 2 || q < 0x80000000u) cell_w<L>(P, q, n, ninv);
-            else { cell_w<L>(P, q, n, ninv); cond_sub_chain(P, n); }
+            const bool wide = L != 2 && q >= 0x80000000u;
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                cell_w<L>(P[j], q, n[j], ninv[j]);
+                if (wide) cond_sub_chain(P[j], n[j]);
+            }
             ++cells;
         }
     }
     if (h_cur) {
-        fold_pow<L>(A, P, h_cur, n, ninv);
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], h_cur, n[j], ninv[j]);
         defA += (u128)h_cur * (32ull * cells + 32 * L);
     }
     for (uint32_t k = 0; k < sb; ++k) {               // A^(2^sb)
-        A = mont_mul<L>(A, A, n, ninv);
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) A[j] = mont_mul<L>(A[j], A[j], n[j], ninv[j]);
         defA = 2 * defA + 32 * L;
     }
 
     // ---- windows over the low bits, top window first ----
-    Res<L> acc;
-    set_small<L>(acc, 1);
-    u128 defacc = 0;
-    for (int j = (int)nwin - 1; j >= 0; --j) {
-        Res<L> B[NBK];
+    Res<L> acc[RPT];
 #pragma unroll
-        for (int d = 0; d < NBK; ++d) set_small<L>(B[d], 1);
+    for (int j = 0; j < RPT; ++j) set_small<L>(acc[j], 1);
+    u128 defacc = 0;
+    for (int w = (int)nwin - 1; w >= 0; --w) {
+        Res<L> B[RPT][NBK];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j)
+#pragma unroll
+            for (int d = 0; d < NBK; ++d) set_small<L>(B[j][d], 1);
         __syncthreads();
         for (uint32_t k = lt; k <= NBK; k += tps) scnt[g][k] = 0;
         for (uint32_t ch = 0; ch < nchunks; ++ch) {
             __syncthreads();
             const uint64_t cb = c0 + (uint64_t)ch * KG;
+            const uint32_t nh = (has_split && cb < c1) ? (uint32_t)(c1 - cb < KG ? c1 - cb : KG) : 0;
+            if (SORT) {
+                for (uint32_t k = lt; k <= NBK; k += tps) scur[g][k] = 0;
+                __syncthreads();
+            }
             for (uint32_t k = lt; k < KG; k += tps) {
                 if (has_split && cb + k < c1) {
                     const uint32_t q = cols[cb + k];
-                    const uint32_t dg = (uint32_t)(((legendre(T, q) & lmask) >> (DW * j)) & NBK);
+                    const uint32_t dg = (uint32_t)(((legendre(T, q) & lmask) >> (DW * w)) & NBK);
                     sq[base + k] = q;
                     sm[base + k] = dg;
-                    atomicAdd(&scnt[g][dg], 1u);
+                    atomicAdd(SORT ? &scur[g][dg] : &scnt[g][dg], 1u);
                 }
             }
             __syncthreads();
-            const uint32_t nh = (has_split && cb < c1) ? (uint32_t)(c1 - cb < KG ? c1 - cb : KG) : 0;
-            for (uint32_t k = 0; k < nh; ++k) {
-                const uint32_t d = (uint32_t)sm[base + k];
-                const uint32_t q = sq[base + k];
-                if (d) bucket_cell<L, NBK>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
+            if (SORT) {
+                // exclusive prefix of the digit counts (the scatter cursors), and
+                // the deficit of each bucket's run: 32 per cell, 32L for the fold of X
+                if (lt == 0) {
+                    uint32_t o = 0;
+                    for (int d = 0; d <= NBK; ++d) {
+                        const uint32_t c = scur[g][d];
+                        scur[g][d] = o;
+                        o += c;
+                        scnt[g][d] += c + (c >= 2 ? (uint32_t)L : 0u);
+                    }
+                }
+                __syncthreads();
+                for (uint32_t k = lt; k < nh; k += tps) {
+                    const uint32_t dg = (uint32_t)sm[base + k];
+                    ss[base + atomicAdd(&scur[g][dg], 1u)] = sq[base + k];
+                }
+                __syncthreads();
+                // after the scatter scur[d] is the end of digit d's run
+                Res<L> X[RPT];
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) set_small<L>(X[j], 1);
+#pragma unroll
+                for (int d = 1; d <= NBK; ++d) {
+                    const uint32_t k0 = scur[g][d - 1], k1 = scur[g][d];
+                    uint32_t k = k0;
+                    for (; k + 1 < k1; k += 2) {
+                        const uint32_t qa = ss[base + k], qb = ss[base + k + 1];
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            cell_w<L>(B[j][d - 1], qa, n[j], ninv[j]);
+                            cell_w<L>(X[j], qb, n[j], ninv[j]);
+                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][d - 1], n[j]);
+                            if (L != 2 && qb >= 0x80000000u) cond_sub_chain(X[j], n[j]);
+                        }
+                    }
+                    if (k < k1) {
+                        const uint32_t qa = ss[base + k];
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            cell_w<L>(B[j][d - 1], qa, n[j], ninv[j]);
+                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][d - 1], n[j]);
+                        }
+                    }
+                    if (k1 - k0 >= 2) {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            B[j][d - 1] = mont_mul<L>(B[j][d - 1], X[j], n[j], ninv[j]);
+                            set_small<L>(X[j], 1);
+                        }
+                    }
+                }
+            } else {
+                for (uint32_t k = 0; k < nh; ++k) {
+                    const uint32_t d = (uint32_t)sm[base + k];
+                    const uint32_t q = sq[base + k];
+                    if (d) bucket_cell<L, NBK, RPT>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
+                }
             }
         }
         // R = prod_d B_d^d by running products from the top bucket down
         __syncthreads();
-        Res<L> S = B[NBK - 1], R = B[NBK - 1];
         u128 defS = (u128)32 * scnt[g][NBK], defR = defS;
 #pragma unroll
         for (int d = NBK - 2; d >= 0; --d) {
-            S = mont_mul<L>(S, B[d], n, ninv);
             defS += (u128)32 * scnt[g][d + 1] + 32 * L;
-            R = mont_mul<L>(R, S, n, ninv);
             defR += defS + 32 * L;
         }
-        if (j == (int)nwin - 1) {
-            acc = R;
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            Res<L> S = B[j][NBK - 1], R = B[j][NBK - 1];
+#pragma unroll
+            for (int d = NBK - 2; d >= 0; --d) {
+                S = mont_mul<L>(S, B[j][d], n[j], ninv[j]);
+                R = mont_mul<L>(R, S, n[j], ninv[j]);
+            }
+            if (w == (int)nwin - 1) {
+                acc[j] = R;
+            } else {
+                for (int k = 0; k < DW; ++k) acc[j] = mont_mul<L>(acc[j], acc[j], n[j], ninv[j]);
+                acc[j] = mont_mul<L>(acc[j], R, n[j], ninv[j]);
+            }
+        }
+        if (w == (int)nwin - 1) {
             defacc = defR;
         } else {
-            for (int k = 0; k < DW; ++k) {
-                acc = mont_mul<L>(acc, acc, n, ninv);
-                defacc = 2 * defacc + 32 * L;
-            }
-            acc = mont_mul<L>(acc, R, n, ninv);
+            for (int k = 0; k < DW; ++k) defacc = 2 * defacc + 32 * L;
             defacc += defR + 32 * L;
         }
     }
-    Res<L> res = A;
     u128 def = defA;
-    if (nwin) {
-        res = mont_mul<L>(A, acc, n, ninv);
-        def = defA + defacc + 32 * L;
-    }
-    if (live) {
-        uint4 o;
-        o.x = res.w[0];
-        o.y = res.w[1];
-        o.z = L > 2 ? res.w[2 < L ? 2 : 0] : 0;
-        o.w = L > 3 ? res.w[3 < L ? 3 : 0] : 0;
-        part[bk.part_base + (uint64_t)s * bk.nrows + r] = o;
+    if (nwin) def = defA + defacc + 32 * L;
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        Res<L> res = A[j];
+        if (nwin) res = mont_mul<L>(A[j], acc[j], n[j], ninv[j]);
+        if (live[j]) {
+            uint4 o;
+            o.x = res.w[0];
+            o.y = res.w[1];
+            o.z = L > 2 ? res.w[2 < L ? 2 : 0] : 0;
+            o.w = L > 3 ? res.w[3 < L ? 3 : 0] : 0;
+            part[bk.part_base + (uint64_t)s * bk.nrows + it.row0 + lt + j * tps] = o;
+        }
     }
     if (has_split && it.row0 == 0 && lt == 0) {
         Deficit dd;
@@ -1529,21 +1626,38 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
     else if (variant == 2) launch_sweep_v<2>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
     else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
 }
-void launch_sweep_dense(int L, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
-                        const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs, cudaStream_t st) {
+void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
+                        const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
+                        cudaStream_t st) {
     if (!nitems) return;
-    // window width and CTAs per SM (measured on B200): 4-bit windows at
-    // 2 CTAs/SM for 2- and 3-limb residues, 3-bit windows at 3 CTAs/SM for
-    // 4-limb ones (fewer bucket registers, more warps); WL_DENSE_CFG overrides
+    // tuning knobs (measured defaults): WL_DENSE_SORT (digit-sorted windows),
+    // WL_DENSE_HSTEP (columns per change of the high exponent part),
+    // WL_DENSE_CFG (window width and CTAs per SM of the unsorted kernel)
+    static const int env_sort = getenv("WL_DENSE_SORT") ? atoi(getenv("WL_DENSE_SORT")) : 1;
+    static const int env_hstep = getenv("WL_DENSE_HSTEP") ? atoi(getenv("WL_DENSE_HSTEP")) : 8;
     static const int env_cfg = getenv("WL_DENSE_CFG") ? atoi(getenv("WL_DENSE_CFG")) : 0;
-    const int cfg = env_cfg ? env_cfg : (L == 4 ? 33 : 42);
-#define WL_D(LL, MB, DWB) k_sweep_dense<LL, MB, DWB><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs)
-    if (cfg == 33) {
-        if (L == 2) WL_D(2, 3, 3); else if (L == 3) WL_D(3, 3, 3); else WL_D(4, 3, 3);
-    } else if (cfg == 32) {
-        if (L == 2) WL_D(2, 2, 3); else if (L == 3) WL_D(3, 2, 3); else WL_D(4, 2, 3);
+    const uint32_t hstep = (uint32_t)(env_hstep > 0 ? env_hstep : 8);
+#define WL_D(LL, MB, DWB, RR, SS) \
+    k_sweep_dense<LL, MB, DWB, RR, SS><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs, hstep)
+    if (rpt == 2) {
+        if (L == 2) WL_D(2, 2, 3, 2, 0); else if (L == 3) WL_D(3, 2, 3, 2, 0); else WL_D(4, 2, 3, 2, 0);
+    } else if (env_sort) {
+        // digit-sorted windows: 3-bit windows at 3 CTAs/SM (WL_DENSE_CFG=42:
+        // 4-bit windows at 2 CTAs/SM)
+        if (env_cfg == 42) {
+            if (L == 2) WL_D(2, 2, 4, 1, 1); else if (L == 3) WL_D(3, 2, 4, 1, 1); else WL_D(4, 2, 4, 1, 1);
+        } else {
+            if (L == 2) WL_D(2, 3, 3, 1, 1); else if (L == 3) WL_D(3, 3, 3, 1, 1); else WL_D(4, 3, 3, 1, 1);
+        }
     } else {
-        if (L == 2) WL_D(2, 2, 4); else if (L == 3) WL_D(3, 2, 4); else WL_D(4, 2, 4);
+        // 4-bit windows at 2 CTAs/SM for 2- and 3-limb residues, 3-bit windows
+        // at 3 CTAs/SM for 4-limb ones
+        const int cfg = env_cfg ? env_cfg : (L == 4 ? 33 : 42);
+        if (cfg == 33) {
+            if (L == 2) WL_D(2, 3, 3, 1, 0); else if (L == 3) WL_D(3, 3, 3, 1, 0); else WL_D(4, 3, 3, 1, 0);
+        } else {
+            if (L == 2) WL_D(2, 2, 4, 1, 0); else if (L == 3) WL_D(3, 2, 4, 1, 0); else WL_D(4, 2, 4, 1, 0);
+        }
     }
 #undef WL_D
 }

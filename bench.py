@@ -111,6 +111,20 @@ def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1, m
     raise SystemExit(f"unknown workload {name}")
 
 
+def merge_over_ranks(dist, times, counts, device="cuda"):
+    """Whole-job figures: the max over ranks of each timing and the sum over
+    ranks of each work count.  Every rank takes part, in the same order; with
+    no process group the values are returned as they are."""
+    if dist is None:
+        return list(times), list(counts)
+    import torch
+    t = torch.tensor(list(times), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor(list(counts), dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return t.tolist(), c.tolist()
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
@@ -192,32 +206,47 @@ def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    ranges, q_cap, desc = workload(args.workload, 0, 1, args.width, args.qcap)
-    lo, hi = ranges[0]
+    ranges, q_cap, desc = workload(args.workload, 0, 1, args.width, args.qcap, args.max_width)
+    lo, hi = max(ranges, key=lambda r: r[1] - r[0])
     import oracle
     oracle.build()
     cores = int(oracle.lib().orc_threads())
     n = len(oracle.list_primes(lo, hi))
-    # a step: `k` evenly spaced rows of the workload with all columns (~5 s)
+    # a step: `k` evenly spaced rows of the workload with all their columns,
+    # k doubled from the core count until a step takes about 5 s, so that the
+    # column sieve each step repeats does not dominate
     k = max(1, cores)
-    sel = list(range(0, n, max(1, n // k)))[:k]
+    while True:
+        sel = list(range(0, n, max(1, n // k)))[:k]
+        t0 = time.perf_counter()
+        oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        if time.perf_counter() - t0 > 5.0 or k >= n or k >= 64 * cores:
+            break
+        k *= 2
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        rows, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
-    value = len(sel) * len(times) / tot
+    if q_cap:
+        # the capped sweep's unit: column cells (sieving primes q <= T, q < q_cap) of the sampled rows
+        per_class = [oracle.count_primes_below(min(t, q_cap - 1) + 1) if t else 0 for t in targets]
+        work = sum(per_class[int(rows["type"][i])] for i in sel)
+        metric, unit = "128-bit mulmods/s (capped column sweep)", "mulmods/s"
+    else:
+        work, metric, unit = len(sel), "primes tested/s", "primes/s"
+    value = work * len(times) / tot
     line = {
-        "metric": "primes tested/s", "value": value, "unit": "primes/s", "impl": "reference",
+        "metric": metric, "value": value, "unit": unit, "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": desc, "sample_rows_per_step": len(sel), "rows_in_workload": n},
-        "cpu_baseline": {"value": value, "unit": "primes/s", "cores": cores, "kind": "port",
-                         "sample": f"{len(sel)} of {n} primes per step, evenly spaced"},
-        "e2e": {"value": value, "unit": "primes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
+                         "sample": f"{len(sel)} of {n} primes per step, evenly spaced, q_cap={q_cap}"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -270,13 +299,7 @@ def run_serving(args, rank, world, local):
     rows = sum(i.tested for i in infos)
     busy_s = ((st1["ms_steps"] - st0["ms_steps"]) + (st1["ms_admit"] - st0["ms_admit"])) / 1e3
     lat = np.array([i.ms_latency for i in infos])
-    if dist:
-        t = torch.tensor([wall, busy_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        wall, busy_s = t.tolist()
-        c = torch.tensor([cells, rows], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        cells, rows = c.tolist()
+    (wall, busy_s), (cells, rows) = merge_over_ranks(dist, [wall, busy_s], [cells, rows])
     line = {
         "metric": "128-bit mulmods/s (capped column sweep, serving)", "value": cells / busy_s,
         "unit": "mulmods/s", "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup),
@@ -397,15 +420,8 @@ def main():
     launches = sum(s.kernel_launches for s in stats)
     h2d = stats[-1].h2d_bytes
     d2h = stats[-1].d2h_bytes
-    if dist:
-        t = torch.tensor([tot_dev, tot_wall, sweep_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_dev, tot_wall, sweep_max = t.tolist()
-        c = torch.tensor([tested, cells, launches], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        tested_all, cells_all, _ = c.tolist()
-    else:
-        tested_all, cells_all = tested, cells
+    (tot_dev, tot_wall, _), (tested_all, cells_all, _) = merge_over_ranks(
+        dist, [tot_dev, tot_wall, sweep_s], [tested, cells, launches])
 
     full = q_cap == 0
     achieved = cells * OPS_PER_CELL[L] / sweep_s / 1e12

@@ -98,7 +98,8 @@ assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
-           "wl_batch", "wl_drop_columns", "wl_parse_uint64", "wl_probe", "wl_column_product_noalloc",
+           "wl_batch", "wl_rows_from", "wl_search_from", "wl_drop_columns", "wl_parse_uint64", "wl_probe",
+           "wl_column_product_noalloc",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
 PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
@@ -132,6 +133,10 @@ def load_library(path: str = LIB_PATH):
     L.wl_batch.argtypes = [vp, ctypes.POINTER(_Range), sz, u64, ctypes.POINTER(_RangeResult),
                            ctypes.POINTER(_Result), sz, ctypes.POINTER(sz), ctypes.POINTER(_Stats)]
     L.wl_batch.restype = ctypes.c_int
+    L.wl_rows_from.argtypes = [vp, u64, u64, u64, u64, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(_Stats)]
+    L.wl_rows_from.restype = ctypes.c_int
+    L.wl_search_from.argtypes = [vp, u64, u64, u64, vp, ctypes.POINTER(_Result), sz, ctypes.POINTER(_Stats)]
+    L.wl_search_from.restype = ctypes.c_int
     L.wl_parse_uint64.argtypes = [ctypes.POINTER(u64), ctypes.c_char_p, u64, u64]
     L.wl_parse_uint64.restype = ctypes.c_int
     L.wl_drop_columns.argtypes = [vp]
@@ -290,6 +295,38 @@ class Engine:
         if rc and rc not in (-5, -6):
             raise WilsonError(rc, "wl_rows")
         return buf[: n.value].copy(), Stats.from_c(st)
+
+    @staticmethod
+    def _init_array(init):
+        if init is None:
+            return None, None
+        a = np.ascontiguousarray(np.stack([np.asarray(init["s0"], dtype=np.uint64),
+                                           np.asarray(init["s1"], dtype=np.uint64)], axis=1))
+        return a, a.ctypes.data
+
+    def rows_from(self, pmin: int, pmax: int, q_lo: int, q_cap: int = 0, init=None) -> Tuple[np.ndarray, Stats]:
+        """Rows over the sieving primes q in [q_lo, q_cap), continuing from the
+        running products `init` (rows of an earlier capped call, or None)."""
+        keep, ptr = self._init_array(init)
+        n = ctypes.c_size_t(0)
+        st = _Stats()
+        cap = (pmax - pmin) // 2 + 2
+        buf = np.zeros(cap, dtype=ROW_DTYPE)
+        rc = self._L.wl_rows_from(self._ctx, pmin, pmax, q_lo, q_cap, ptr, buf.ctypes.data, cap, ctypes.byref(n),
+                                  ctypes.byref(st))
+        if rc and rc not in (-5, -6):
+            raise WilsonError(rc, "wl_rows_from")
+        return buf[: n.value].copy(), Stats.from_c(st)
+
+    def search_from(self, pmin: int, pmax: int, q_lo: int, init=None, cap: int = 1 << 16) -> SearchResult:
+        keep, ptr = self._init_array(init)
+        res = (_Result * cap)()
+        st = _Stats()
+        rc = self._L.wl_search_from(self._ctx, pmin, pmax, q_lo, ptr, res, cap, ctypes.byref(st))
+        if rc:
+            raise WilsonError(rc, "wl_search_from")
+        out = [(res[i].p, res[i].value) for i in range(min(st.results, cap))]
+        return SearchResult(out, st.checksum, Stats.from_c(st))
 
     def batch(self, ranges: Sequence[Tuple[int, int]], q_cap: int = 0, cap: int = 1 << 20):
         n = len(ranges)

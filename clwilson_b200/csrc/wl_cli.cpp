@@ -9,9 +9,14 @@
 //          init_data.xml (<gpu_device_num>) or defaults to 0
 //   -h     help
 // Writes results.txt (truncated at the start, one line per result, then the checksum
-// line) exactly as the reference does.  All arithmetic runs in libwilson.so.
+// line) exactly as the reference does.  Long searches run in pieces of columns and
+// checkpoint every minute to stateA.ckp / stateB.ckp in the reference's format
+// (cl_wilson.cpp:110-288), so a search resumes from its last checkpoint -- also one
+// written by the reference program.  All arithmetic runs in libwilson.so.
 #include <getopt.h>
+#include <algorithm>
 #include <cinttypes>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -23,6 +28,17 @@
 
 static const char* RESULT_FILENAME = "results.txt";
 static const char* GOOD_RES_FILENAME = "goodWilsonResults.txt";
+static const char* STATE_FILENAME_A = "stateA.ckp";
+static const char* STATE_FILENAME_B = "stateB.ckp";
+
+typedef unsigned __int128 u128;
+
+// The checkpoint header, byte for byte the reference's workStatus (cl_wilson.h:22-25).
+struct WorkStatus {
+    uint64_t pmin, pmax, currp, trickle, state_sum, totalcount;
+    uint32_t tpcount, done;
+};
+static_assert(sizeof(WorkStatus) == 56, "workStatus layout");
 
 struct Opts {
     uint64_t pmin = 0, pmax = 0;
@@ -121,7 +137,10 @@ struct RunResult {
     int rc = 0;
 };
 
-static RunResult run_search(wl_ctx* ctx, const Opts& o, bool verbose) {
+// The search from column q_lo on (init: the rows' running products below q_lo,
+// two digits per row; NULL with q_lo = 2 for a search from the start).
+static RunResult run_search(wl_ctx* ctx, const Opts& o, bool verbose, uint64_t q_lo = 2,
+                            const uint64_t* init = nullptr) {
     RunResult rr;
     // the whole row set (needed for -r) or just the result lines
     wl_stats st;
@@ -129,7 +148,7 @@ static RunResult run_search(wl_ctx* ctx, const Opts& o, bool verbose) {
     if (o.result_test) {
         size_t cap = (o.pmax - o.pmin) / 2 + 2, n = 0;
         rows.resize(cap);
-        rr.rc = wl_rows(ctx, o.pmin, o.pmax, 0, rows.data(), cap, &n, &st);
+        rr.rc = wl_rows_from(ctx, o.pmin, o.pmax, q_lo, 0, init, rows.data(), cap, &n, &st);
         rows.resize(n);
         for (const wl_row& r : rows) {
             const uint64_t negq = r.p - r.quot, sm = r.quot <= negq ? r.quot : negq;
@@ -138,10 +157,10 @@ static RunResult run_search(wl_ctx* ctx, const Opts& o, bool verbose) {
         }
     } else {
         std::vector<wl_result> res(1 << 16);
-        rr.rc = wl_search(ctx, o.pmin, o.pmax, 0, res.data(), res.size(), &st);
+        rr.rc = wl_search_from(ctx, o.pmin, o.pmax, q_lo, init, res.data(), res.size(), &st);
         if (rr.rc == WL_ERR_CAPACITY) {
             res.resize(st.results);
-            rr.rc = wl_search(ctx, o.pmin, o.pmax, 0, res.data(), res.size(), &st);
+            rr.rc = wl_search_from(ctx, o.pmin, o.pmax, q_lo, init, res.data(), res.size(), &st);
         }
         res.resize(st.results);
         rr.results = res;
@@ -210,10 +229,194 @@ static void write_results_file(const RunResult& rr) {
     if (fclose(f) != 0) fail("Cannot close results.txt !!!\n");
 }
 
+// ---- checkpoints (cl_wilson.cpp:110-288) ----------------------------------------
+// The reference keeps each row's running product in Montgomery form with
+// R = 2^64 mod p^2, as base-p digits (kernels/common.cl:120-130); the engine
+// returns plain values.  Conversion: multiply or divide by 2^64 mod p^2.
+static void to_reference(uint64_t p, uint64_t s0, uint64_t s1, uint64_t* r0, uint64_t* r1) {
+    const u128 n = (u128)p * p;
+    u128 x = (u128)s1 * p + s0;
+    for (int i = 0; i < 64; ++i) {
+        x <<= 1;
+        if (x >= n) x -= n;
+    }
+    *r0 = (uint64_t)(x % p);
+    *r1 = (uint64_t)(x / p);
+}
+
+static void from_reference(uint64_t p, uint64_t r0, uint64_t r1, uint64_t* s0, uint64_t* s1) {
+    const u128 n = (u128)p * p;
+    u128 x = ((u128)r1 * p + r0) % n;
+    for (int i = 0; i < 64; ++i) x = (x & 1) ? (x + n) >> 1 : x >> 1;
+    *s0 = (uint64_t)(x % p);
+    *s1 = (uint64_t)(x / p);
+}
+
+static uint64_t state_checksum(const WorkStatus& st, const std::vector<uint64_t>& res) {
+    uint64_t sum = st.pmin + st.pmax + st.currp + st.trickle + st.totalcount + st.tpcount + st.done;
+    for (uint32_t i = 0; i < st.tpcount; ++i) sum += res[2 * i] + res[2 * i + 1];
+    return sum;
+}
+
+// write_state: the header then tpcount residue pairs, alternating A and B
+static void write_state(bool& write_a_next, WorkStatus& st, const std::vector<uint64_t>& ref_res) {
+    st.state_sum = state_checksum(st, ref_res);
+    const char* name = write_a_next ? STATE_FILENAME_A : STATE_FILENAME_B;
+    FILE* out = fopen(name, "wb");
+    if (!out) {
+        fprintf(stderr, "Cannot open %s !!!\n", name);
+        return;
+    }
+    bool ok = fwrite(&st, sizeof(WorkStatus), 1, out) == 1 &&
+              fwrite(ref_res.data(), 16, st.tpcount, out) == st.tpcount;
+    if (!ok) fprintf(stderr, "Cannot write checkpoint to file. Continuing...\n");
+    if (fclose(out) == 0 && ok) write_a_next = !write_a_next;
+}
+
+// read_state: 0 no usable checkpoint, 1 resume (st, ref_res filled), 2 finished
+static int read_one_state(const char* name, const WorkStatus& want, WorkStatus& st, std::vector<uint64_t>& res) {
+    FILE* in = fopen(name, "rb");
+    if (!in) return 0;
+    int r = 1;
+    res.assign(2 * (size_t)want.tpcount, 0);
+    if (fread(&st, sizeof(WorkStatus), 1, in) != 1 || fread(res.data(), 16, want.tpcount, in) != want.tpcount) {
+        fprintf(stderr, "Cannot parse %s !!!\n", name);
+        printf("Cannot parse %s !!!\n", name);
+        r = 0;
+    } else if (st.tpcount != want.tpcount || st.pmin != want.pmin || st.pmax != want.pmax) {
+        fprintf(stderr, "Invalid checkpoint file %s !!!\n", name);
+        printf("Invalid checkpoint file %s !!!\n", name);
+        r = 0;
+    } else if (st.done) {
+        r = 2;
+    } else if (state_checksum(st, res) != st.state_sum) {
+        fprintf(stderr, "Checksum error in %s !!!\n", name);
+        printf("Checksum error in %s !!!\n", name);
+        r = 0;
+    }
+    fclose(in);
+    return r;
+}
+
+static int read_state(bool& write_a_next, WorkStatus& st, std::vector<uint64_t>& ref_res) {
+    WorkStatus a, b;
+    std::vector<uint64_t> ra, rb;
+    const int ga = read_one_state(STATE_FILENAME_A, st, a, ra);
+    if (ga == 2) return 2;
+    const int gb = read_one_state(STATE_FILENAME_B, st, b, rb);
+    if (gb == 2) return 2;
+    if (ga == 1 && (gb != 1 || a.currp > b.currp)) {
+        st = a;
+        ref_res.swap(ra);
+        write_a_next = false;
+        return 1;
+    }
+    if (gb == 1) {
+        st = b;
+        ref_res.swap(rb);
+        write_a_next = true;
+        return 1;
+    }
+    return 0;
+}
+
+static double prime_count_estimate(double x) { return x < 17 ? 7 : x / std::log(x); }
+
 static int search(wl_ctx* ctx, const Opts& o) {
     setup_search(o);
     time_t t0 = time(nullptr);
-    RunResult rr = run_search(ctx, o, true);
+    // the test primes and class targets: the rows with no columns multiplied in
+    size_t cap = (o.pmax - o.pmin) / 2 + 2, n = 0;
+    std::vector<wl_row> rows(cap);
+    wl_stats st0;
+    int rc = wl_rows(ctx, o.pmin, o.pmax, 2, rows.data(), cap, &n, &st0);
+    if (rc) {
+        fprintf(stderr, "error: %s\n", wl_strerror(rc));
+        printf("error: %s\n", wl_strerror(rc));
+        return EXIT_FAILURE;
+    }
+    rows.resize(n);
+    const uint64_t maxtarget = std::max(st0.targets[0], std::max(st0.targets[1], st0.targets[2]));
+    WorkStatus ws;
+    memset(&ws, 0, sizeof(ws));
+    ws.pmin = o.pmin;
+    ws.pmax = o.pmax;
+    ws.currp = 2;
+    ws.tpcount = (uint32_t)n;
+    std::vector<uint64_t> res(2 * n), ref(2 * n);
+    for (size_t i = 0; i < n; ++i) { res[2 * i] = 1; res[2 * i + 1] = 0; }
+    bool write_a_next = true;
+    const int rsr = read_state(write_a_next, ws, ref);
+    if (rsr == 2) {
+        printf("Workunit complete.\n");
+        fprintf(stderr, "Workunit complete.\n");
+        return EXIT_SUCCESS;
+    }
+    if (rsr == 1) {
+        printf("Resuming search from checkpoint. Current P: %" PRIu64 "\n", ws.currp);
+        fprintf(stderr, "Resuming search from checkpoint. Current P: %" PRIu64 "\n", ws.currp);
+        for (size_t i = 0; i < n; ++i) from_reference(rows[i].p, ref[2 * i], ref[2 * i + 1], &res[2 * i], &res[2 * i + 1]);
+    } else {
+        FILE* f = fopen(RESULT_FILENAME, "w");
+        if (!f) fail("Cannot open results.txt !!!\n");
+        fclose(f);
+        ws.trickle = (uint64_t)time(nullptr);
+    }
+
+    // pieces of about 10 s of work while more than about 20 s remain, a
+    // checkpoint at most once a minute, then the last piece (the remaining
+    // columns, the tail and the lift).  For tests: WL_CKPT_PIECE fixes the
+    // piece width (integers), WL_CKPT_INTERVAL the seconds between
+    // checkpoints, and WL_CKPT_STOP=k ends the program (exit status 3) after
+    // k pieces and a checkpoint, as an interrupted run would.
+    const uint64_t fixed_piece = getenv("WL_CKPT_PIECE") ? strtoull(getenv("WL_CKPT_PIECE"), nullptr, 0) : 0;
+    const int interval = getenv("WL_CKPT_INTERVAL") ? atoi(getenv("WL_CKPT_INTERVAL")) : 60;
+    const int stop_after = getenv("WL_CKPT_STOP") ? atoi(getenv("WL_CKPT_STOP")) : 0;
+    double rate = 1.0e11;   // column cells per second, refined by measurement
+    time_t ckpt_last = time(nullptr);
+    bool chunked = false;
+    int pieces = 0;
+    while (ws.currp <= maxtarget) {
+        uint64_t stop;
+        if (fixed_piece) {
+            if (maxtarget + 1 - ws.currp <= fixed_piece) break;
+            stop = ws.currp + fixed_piece;
+        } else {
+            const double left =
+                (double)n * (prime_count_estimate((double)maxtarget) - prime_count_estimate((double)ws.currp));
+            if (left <= rate * 20.0) break;
+            const double want = rate * 10.0 / (double)n;   // primes per piece
+            const double lnx = std::log(std::max((double)ws.currp, 17.0));
+            stop = ws.currp + (uint64_t)std::max(1.0e6, want * lnx);
+            if (stop > maxtarget) stop = maxtarget + 1;
+        }
+        const time_t tc = time(nullptr);
+        wl_stats st;
+        size_t got = 0;
+        std::vector<wl_row> part(n);
+        rc = wl_rows_from(ctx, o.pmin, o.pmax, ws.currp, stop, res.data(), part.data(), n, &got, &st);
+        if (rc || got != n) {
+            fprintf(stderr, "error: %s\n", wl_strerror(rc ? rc : WL_ERR_ARG));
+            printf("error: %s\n", wl_strerror(rc ? rc : WL_ERR_ARG));
+            return EXIT_FAILURE;
+        }
+        for (size_t i = 0; i < n; ++i) { res[2 * i] = part[i].s0; res[2 * i + 1] = part[i].s1; }
+        const double secs = st.ms_device / 1e3;
+        if (secs > 0.5 && st.cells) rate = std::min(rate * 4.0, (double)st.cells / secs);
+        ws.currp = stop;
+        ws.totalcount = st.pi_maxtarget;
+        chunked = true;
+        ++pieces;
+        const bool stopping = stop_after > 0 && pieces >= stop_after;
+        if ((int)(time(nullptr) - ckpt_last) >= interval || stopping) {
+            ckpt_last = time(nullptr);
+            for (size_t i = 0; i < n; ++i) to_reference(part[i].p, res[2 * i], res[2 * i + 1], &ref[2 * i], &ref[2 * i + 1]);
+            write_state(write_a_next, ws, ref);
+            printf("Checkpoint, Current P: %" PRIu64 "\n", ws.currp);
+        }
+        if (stopping) return 3;
+    }
+    RunResult rr = run_search(ctx, o, true, ws.currp, (chunked || rsr == 1) ? res.data() : nullptr);
     if (rr.rc) {
         fprintf(stderr, "error: %s\n", wl_strerror(rr.rc));
         printf("error: %s\n", wl_strerror(rr.rc));
@@ -224,6 +427,11 @@ static int search(wl_ctx* ctx, const Opts& o) {
         else printf("%" PRIu64 " is a Near-Wilson prime %+d\n", r.p, r.value);
     }
     write_results_file(rr);
+    // the finished workunit (read_state reports it complete)
+    ws.done = 1;
+    ws.currp = maxtarget + 1;
+    for (size_t i = 0; i < n; ++i) to_reference(rows[i].p, res[2 * i], res[2 * i + 1], &ref[2 * i], &ref[2 * i + 1]);
+    write_state(write_a_next, ws, ref);
     fprintf(stderr, "Search complete. Results: %zu, total power table primes generated %" PRIu64 ", removed 0 PRPs\n",
             rr.results.size(), rr.pi_maxtarget);
     printf("Search finished in %d sec.\n", (int)(time(nullptr) - t0));

@@ -222,7 +222,7 @@ static uint64_t isqrt_u64(uint64_t n) {
 
 static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::vector<RowInfo>& ri, uint32_t nrows,
                            const std::vector<uint64_t>& keys_host_order, uint64_t big_need, uint64_t maxt0, bool full,
-                           uint64_t qcap, uint64_t* pi_big) {
+                           uint64_t qcap, uint64_t q_lo, uint64_t* pi_big) {
     (void)keys_host_order;
     cudaStream_t s3 = c->st3;
     CK(cudaStreamWaitEvent(s3, c->rows_ready, 0));   // row tables and moduli
@@ -278,6 +278,7 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
     std::vector<SweepItem> all;
     for (uint64_t w0 = LO; w0 < big_need; w0 += WIN) {
         const uint64_t w1 = std::min(w0 + WIN, big_need);
+        if (w1 <= q_lo) continue;   // a resumed search starts at q_lo
         const uint32_t nseg = (uint32_t)((w1 - w0 + BIG_SPAN - 1) / BIG_SPAN);
         const uint32_t ncta = (nseg + SPC - 1) / SPC;
         RC(ensure(c->bbitmap, (size_t)nseg * BIG_WORDS * 4));
@@ -286,6 +287,10 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
         launch_sieve_big(w0, w1, nseg, SPC, base, nbase, as<uint32_t>(c->boffs), as<uint32_t>(c->bbitmap),
                          as<uint32_t>(c->bsegcount), s3);
         c->launches++;
+        if (q_lo > w0) {
+            launch_clear_below(as<uint32_t>(c->bbitmap), w0, q_lo, (uint64_t)nseg * BIG_WORDS, s3);
+            c->launches++;
+        }
         if (maxt0 >= w0) {
             launch_count_bits(as<uint32_t>(c->bbitmap), w0, (uint64_t)nseg * BIG_WORDS, maxt0,
                               as<unsigned long long>(c->wcounts), s3);
@@ -312,6 +317,7 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
             x.ncols = (uint32_t)nw[b];
             x.cdense = 0;
             x.ndense = 0;
+            x.cbase = 0;
             x.part_base = part_total;
             x.def_base = def_total;
             if (!nw[b]) { x.nsplit = 0; continue; }
@@ -448,7 +454,11 @@ static int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::ve
     return 0;
 }
 
-static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qcap, RunOut& out, wl_stats* st) {
+// Columns q in [q_lo, q_cap) (q_cap = 0: through the class target, then the
+// tail and the lift); init: the rows' running products before q_lo, two
+// digits (s0, s1) per row in output order, or NULL for 1.
+static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qcap, RunOut& out, wl_stats* st,
+                      uint64_t q_lo = 2, const uint64_t* init = nullptr) {
     const bool full = (qcap == 0);
     c->launches = 0;
     c->h2d = c->d2h = 0;
@@ -529,6 +539,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         uint64_t qd = q >= 1.8e19 ? ~0ull : (uint64_t)q;
         keys.push_back(std::min<uint64_t>(qd, keys[i]));
     }
+    if (q_lo > 2) keys.push_back(q_lo - 1);   // columns already multiplied in (init)
     RC(ensure(c->keys, keys.size() * 8));
     RC(ensure(c->counts, keys.size() * 8));
     CK(cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st));
@@ -542,7 +553,18 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     c->h2d += keys.size() * 8;
     c->d2h += keys.size() * 8;
     out.pi_maxtarget = ncol[nb];
-    const uint64_t* ndn = ncol.data() + nb + 1;   // dense column counts per bucket
+    uint64_t* ndn = ncol.data() + nb + 1;   // dense column counts per bucket
+    // a search resumed at q_lo: each bucket's columns start at cb_lo[i] (the
+    // primes below q_lo); from here on ncol and ndn count columns from there
+    std::vector<uint64_t> cb_lo(nb, 0);
+    if (q_lo > 2) {
+        const uint64_t c_lo = ncol[2 * nb + 1];
+        for (size_t i = 0; i < nb; ++i) {
+            cb_lo[i] = std::min(c_lo, ncol[i]);
+            ndn[i] = ndn[i] > cb_lo[i] ? ndn[i] - cb_lo[i] : 0;
+            ncol[i] -= cb_lo[i];
+        }
+    }
 
     // ---- 4. device layout: rows, buckets, splits, items ------------------------
     std::vector<Bucket> db(hb.size());
@@ -564,6 +586,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
     std::vector<uint64_t> dkeys;                 // interior dense boundaries (values), all buckets
     std::vector<uint32_t> dkeys_bucket_start, dkeys_n;
+    std::vector<char> dequal;                    // per bucket (device order): equal dense splits
     uint32_t row = 0;
     uint64_t part_total = 0;
     uint32_t def_total = 0;
@@ -641,14 +664,15 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         b.cdense = (uint32_t)nd;
         b.ndense = (uint32_t)Sd;
         b.dstart = (uint32_t)dkeys_bucket_start.size();
-        b.cbase = 0;
+        b.cbase = (uint32_t)cb_lo[i];
         dkeys_bucket_start.push_back((uint32_t)dkeys.size());
         dkeys_n.push_back((uint32_t)Sd);
+        dequal.push_back(cb_lo[i] > 0);
         // interior boundaries at equal cumulative cost (values q: split k ends at
         // q_k), interpolated inside a grid step: there are more splits than grid
         // points when the dense region is long, and a boundary snapped to the
         // grid would leave empty splits next to ones many times too long
-        for (uint64_t k = 1; k < Sd; ++k) {
+        for (uint64_t k = 1; k < Sd && !cb_lo[i]; ++k) {
             const std::vector<double>& cum = dcum[i];
             const std::vector<double>& grid = dgrid[i];
             const double target = cum.back() * (double)k / (double)Sd;
@@ -729,6 +753,12 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             b.dstart = (uint32_t)dsplit.size();
             if (!n) continue;
             dsplit.push_back(0);
+            if (dequal[oi]) {
+                // resumed bucket: equal splits of the remaining dense columns
+                for (uint32_t k = 1; k < n; ++k) dsplit.push_back((uint32_t)((uint64_t)b.cdense * k / n));
+                dsplit.push_back(b.cdense);
+                continue;
+            }
             uint32_t prev = 0;
             for (uint32_t k = 1; k < n; ++k) {
                 uint32_t v = (uint32_t)std::min<uint64_t>(dcounts[k0 + k - 1], b.cdense);
@@ -786,6 +816,23 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
                            cudaMemcpyHostToDevice, c->st));
     c->h2d += db.size() * sizeof(Bucket) + (size_t)nrows * sizeof(RowInfo) + all_items.size() * sizeof(SweepItem);
 
+    // per-row accumulators of the column products (1, or the resumed products)
+    RC(ensure(c->uacc, (size_t)nrows * 16 + 16));
+    RC(ensure(c->udef, db.size() * sizeof(Deficit) + 16));
+    launch_acc_init(nrows, (uint32_t)db.size(), as<uint4>(c->uacc), as<Deficit>(c->udef), c->st);
+    c->launches++;
+    if (init) {
+        // the running products before q_lo, as values s0 + p*s1 < p^2 (deficit 0)
+        std::vector<uint4> iv(nrows);
+        for (uint32_t r = 0; r < nrows; ++r) {
+            const uint64_t s0 = init[2 * row_src[r]], s1 = init[2 * row_src[r] + 1], p = ri[r].p;
+            if (s0 >= p || s1 >= p) return WL_ERR_ARG;
+            const unsigned __int128 v = (unsigned __int128)s1 * p + s0;
+            iv[r] = make_uint4((uint32_t)v, (uint32_t)(v >> 32), (uint32_t)(v >> 64), (uint32_t)(v >> 96));
+        }
+        CK(cudaMemcpyAsync(c->uacc.p, iv.data(), (size_t)nrows * 16, cudaMemcpyHostToDevice, c->st));
+        c->h2d += (size_t)nrows * 16;
+    }
     launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
     c->launches++;
     CK(cudaEventRecord(c->rows_ready, c->st));
@@ -814,10 +861,6 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         CK(cudaStreamWaitEvent(c->st, c->join, 0));
     }
     // merge every row's split partials into its accumulator
-    RC(ensure(c->uacc, (size_t)nrows * 16 + 16));
-    RC(ensure(c->udef, db.size() * sizeof(Deficit) + 16));
-    launch_acc_init(nrows, (uint32_t)db.size(), as<uint4>(c->uacc), as<Deficit>(c->udef), c->st);
-    c->launches++;
     {
         uint32_t maxs = 0;
         for (auto& x : db) maxs = std::max(maxs, x.nsplit);
@@ -840,7 +883,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     bool big = false;
     if (big_need) {
         uint64_t pi_big = 0;
-        RC(run_big_columns(c, db, ri, nrows, keys, big_need, maxt0, full, qcap, &pi_big));
+        RC(run_big_columns(c, db, ri, nrows, keys, big_need, maxt0, full, qcap, q_lo, &pi_big));
         out.pi_maxtarget += pi_big;
         big = true;
     }
@@ -1107,6 +1150,34 @@ int wl_rows(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_cap, wl_row* row
     if (e) return e;
     if (rows && cap < ro.rows.size()) return WL_ERR_CAPACITY;
     return 0;
+}
+
+int wl_rows_from(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_lo, uint64_t q_cap, const uint64_t* init,
+                 wl_row* rows, size_t cap, size_t* nrows, wl_stats* stats) {
+    if (!c || q_lo < 2) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    wl_range r = { pmin, pmax };
+    RunOut ro;
+    RC(run_ranges(c, &r, 1, q_cap, ro, stats, q_lo, init));
+    if (nrows) *nrows = ro.rows.size();
+    if (rows) {
+        const size_t n = std::min(cap, ro.rows.size());
+        memcpy(rows, ro.rows.data(), n * sizeof(wl_row));
+    }
+    int e = summarize(ro, 1, q_cap == 0, nullptr, nullptr, 0, nullptr, stats);
+    if (e) return e;
+    if (rows && cap < ro.rows.size()) return WL_ERR_CAPACITY;
+    return 0;
+}
+
+int wl_search_from(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_lo, const uint64_t* init, wl_result* results,
+                   size_t cap, wl_stats* stats) {
+    if (!c || q_lo < 2) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    wl_range r = { pmin, pmax };
+    RunOut ro;
+    RC(run_ranges(c, &r, 1, 0, ro, stats, q_lo, init));
+    return summarize(ro, 1, true, nullptr, results, cap, nullptr, stats);
 }
 
 int wl_batch(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, wl_range_result* out,
@@ -1451,11 +1522,10 @@ static int serve_step(wl_server* s) {
     wl_ctx* c = s->c;
     struct Work { uint32_t bid; uint64_t c0, len; bool dense; };
     std::vector<Work> work;
-    // the step's descriptor table covers every slot in use: rows of slots
-    // without work this step see nsplit = 0 there
-    uint32_t top = 0;
-    for (uint32_t bid = 0; bid < s->bucket_cap; ++bid)
-        if (s->sb[bid].used) top = bid + 1;
+    // the step's descriptor table covers every slot (a merge over a span of
+    // rows may meet stale bucket ids of freed rows): slots without work this
+    // step have nsplit = 0
+    const uint32_t top = s->bucket_cap;
     size_t nact = 0;
     for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && s->sb[bid].pos < s->sb[bid].ncols;
     if (!nact) return 0;
@@ -1554,19 +1624,28 @@ static int serve_step(wl_server* s) {
         s->ws.launches++;
         ioff += g.items.size();
     }
-    // fold the chunk into the resident running products, one launch per
-    // request (its rows are contiguous and share one limb width)
-    for (SReq* q : s->active) {
-        uint32_t maxs = 0;
-        for (uint32_t bid : q->bids) if (bid < top) maxs = std::max(maxs, bucket_splits[bid]);
+    // fold the chunk into the resident running products: one launch per limb
+    // width over the span of the active requests' rows (rows of buckets
+    // without splits this step, or not in use, are left alone by the kernel)
+    for (int L = 2; L <= 4; ++L) {
+        uint32_t lo = UINT32_MAX, hi = 0, maxs = 0;
+        for (SReq* q : s->active) {
+            if (q->L != L) continue;
+            uint32_t m = 0;
+            for (uint32_t bid : q->bids) if (bid < top) m = std::max(m, bucket_splits[bid]);
+            if (!m) continue;
+            maxs = std::max(maxs, m);
+            lo = std::min(lo, q->r0);
+            hi = std::max(hi, q->r0 + q->nrows);
+        }
         if (!maxs) continue;
         if (maxs >= 64)
-            launch_merge_cta(q->L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
-                             as<uint4>(c->part), as<Deficit>(c->defs), q->r0, q->nrows, as<uint4>(s->acc),
+            launch_merge_cta(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                             as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
                              as<Deficit>(s->bdef), c->st);
         else
-            launch_merge(q->L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
-                         as<uint4>(c->part), as<Deficit>(c->defs), q->r0, q->nrows, as<uint4>(s->acc),
+            launch_merge(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                         as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
                          as<Deficit>(s->bdef), c->st);
         s->ws.launches++;
     }
@@ -1732,6 +1811,7 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
         return WL_ERR_NOMEM;
     }
     cudaMemset(s->pbuckets.p, 0, s->bucket_cap * sizeof(Bucket));
+    cudaMemset(s->info.p, 0, (size_t)s->pool_cap * sizeof(RowInfo));   // bucket 0 for rows never admitted
     s->worker = std::thread(serve_loop, s);
     *out = s;
     return 0;

@@ -1396,6 +1396,18 @@ __global__ void k_count_bits(const uint32_t* __restrict__ bitmap, uint64_t lo, u
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
 }
 
+// Clear the bits of integers below q_lo in a window bitmap (bit b of word w is
+// the odd integer lo + 64w + 1 + 2b): a search that resumes at q_lo takes
+// only the columns from there on.
+__global__ void k_clear_below(uint32_t* __restrict__ bitmap, uint64_t lo, uint64_t q_lo, uint64_t nwords) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwords) return;
+    const uint64_t first = lo + 64 * w + 1;
+    if (first >= q_lo) return;
+    const uint64_t below = (q_lo - first + 1) / 2;           // bits 0 .. below-1 are < q_lo
+    bitmap[w] &= below >= 32 ? 0u : ~((1u << below) - 1u);
+}
+
 // acc[row] *= prod over the window's splits; the bucket's first row also
 // adds the splits' deficits (and 2^(32L) per product) into bdef[bucket]
 template <int L>
@@ -1714,6 +1726,13 @@ void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const R
     if (L == 2) k_merge_cta<2><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
     else if (L == 3) k_merge_cta<3><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
     else k_merge_cta<4><<<nrows, 256, 0, st>>>(buckets, info, mods, part, defs, row_begin, acc, bdef);
+}
+
+void launch_clear_below(uint32_t* bitmap, uint64_t lo, uint64_t q_lo, uint64_t nwords, cudaStream_t st) {
+    if (q_lo <= lo || !nwords) return;
+    const uint64_t lim = (q_lo - lo) / 64 + 1;
+    const uint64_t need = nwords < lim ? nwords : lim;
+    k_clear_below<<<(unsigned)((need + 255) / 256), 256, 0, st>>>(bitmap, lo, q_lo, need);
 }
 
 void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* ipart,

@@ -138,6 +138,21 @@ int wl_batch(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap,
              wl_range_result *out, wl_result *results, size_t cap, size_t *nresults,
              wl_stats *stats);
 
+/* A search in pieces (checkpoint and resume, as the reference's chunked main
+ * loop, cl_wilson.cpp:1856-1929, resumed by read_state, 159-288).
+ * wl_rows_from: as wl_rows with the column product restricted to the sieving
+ * primes q in [q_lo, q_cap) (each class still stops at its target), times the
+ * rows' running products over the primes below q_lo given in `init`: row i
+ * (ascending p, as wl_rows returns them) starts from init[2i] + p*init[2i+1]
+ * (both digits < p; init = NULL: 1).  q_cap = 0 runs to the class targets and
+ * adds the tail and the lift, as wl_rows.  The returned (s0, s1) of a capped
+ * call are the next call's init.  wl_search_from: the last piece, returning
+ * result lines and checksum as wl_search. */
+int wl_rows_from(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_lo, uint64_t q_cap, const uint64_t *init,
+                 wl_row *rows, size_t cap, size_t *nrows, wl_stats *stats);
+int wl_search_from(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_lo, const uint64_t *init,
+                   wl_result *results, size_t cap, wl_stats *stats);
+
 /* Forget the resident column table; the next call sieves it again. */
 void wl_drop_columns(wl_ctx *ctx);
 

@@ -269,7 +269,12 @@ def run_serving(args, rank, world, local):
     reqs = serving_requests(1, args.requests, args.rate, args.max_width)[rank::world]
     L = max(limbs_for(b - 1) for _, a, b in reqs)
     peak_mad = wl.probe("mad", local)
-    srv = wl.Server(local)
+    tuning = None
+    if not args.no_autotune:
+        eng = wl.Engine(local)
+        tuning = eng.autotune([(a, b) for _, a, b in reqs[:64]], q_cap)
+        eng.close()
+    srv = wl.Server(local, tuning=tuning)
 
     def stream(reqs, clk=None):
         ids = []
@@ -320,6 +325,7 @@ def run_serving(args, rank, world, local):
         "server": {k: st1[k] - st0[k] for k in ("steps", "admitted", "completed", "launches")} |
                   {"peak_active": st1["peak_active"], "busy_s": busy_s},
         "gpu_launches": st1["launches"] - st0["launches"],
+        "tuning": tuning if tuning is not None else "defaults",
         "roofline": {"bound": "imad", "peak": peak_mad / 1e12, "unit": "TOP/s", "achieved": None, "frac": None,
                      "traffic": None, "note": "device-busy throughput; see the batched and plain lines for the kernels",
                      "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
@@ -351,6 +357,8 @@ def main():
     ap.add_argument("--qcap", type=int, default=-1,
                     help="column cap q < QCAP (default: the configuration's; only for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default kernel choices instead of timing the variants before the warm-up")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -376,6 +384,14 @@ def main():
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
     ranges, q_cap, desc = workload(args.workload, rank, world, args.width, args.qcap, args.max_width)
     L = max(limbs_for(b - 1) for a, b in ranges)
+    t_tune = time.perf_counter()
+    # tune on the workload itself; the capped plain workloads (over a minute per
+    # step) on the first 1% of their range
+    tune_ranges = ranges
+    if args.workload in ("plain-mid", "plain-top"):
+        tune_ranges = [(a, a + max(20000, (b - a) // 100)) for a, b in ranges]
+    tuning = None if args.no_autotune else eng.autotune(tune_ranges, q_cap)
+    t_tune = time.perf_counter() - t_tune
     peak_mad = wl.probe("mad", local)
     peak_cell = wl.probe("cell%d" % L, local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MiB > L2
@@ -455,6 +471,8 @@ def main():
                 "unit": "primes/s" if full else "mulmods/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "tuning": tuning if tuning is not None else "defaults",
+        "autotune_s": round(t_tune, 2),
         "clocks": clk.summary(),
         "phase_ms_per_step": {k: sum(getattr(s, "ms_" + k) for s in stats) / args.steps
                               for k in ("primes", "sieve", "sweep", "iterate", "finish")},

@@ -70,9 +70,31 @@ class _Stats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double)]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("sparse_variant", ctypes.c_int32 * 3), ("sparse_rpt", ctypes.c_int32 * 3),
+                ("dense_kernel", ctypes.c_int32 * 3), ("dense_hstep", ctypes.c_int32 * 3),
+                ("merge_cta_min", ctypes.c_int32), ("pad", ctypes.c_int32), ("ms", ctypes.c_double * 3)]
+
+    def to_dict(self) -> dict:
+        return {k: (list(getattr(self, k)) if k in ("sparse_variant", "sparse_rpt", "dense_kernel", "dense_hstep", "ms")
+                    else getattr(self, k)) for k, _ in self._fields_ if k != "pad"}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "_Tuning":
+        t = cls()
+        for k, v in d.items():
+            if k in ("sparse_variant", "sparse_rpt", "dense_kernel", "dense_hstep"):
+                setattr(t, k, (ctypes.c_int32 * 3)(*v))
+            elif k == "ms":
+                setattr(t, k, (ctypes.c_double * 3)(*v))
+            elif k == "merge_cta_min":
+                t.merge_cta_min = v
+        return t
+
+
 class _ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("pad", ctypes.c_uint32), ("pool_bytes", ctypes.c_uint64),
-                ("step_cells", ctypes.c_uint64)]
+                ("step_cells", ctypes.c_uint64), ("tuning", ctypes.c_void_p)]
 
 
 class _RequestInfo(ctypes.Structure):
@@ -99,7 +121,7 @@ assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
            "wl_batch", "wl_rows_from", "wl_search_from", "wl_drop_columns", "wl_parse_uint64", "wl_probe",
-           "wl_column_product_noalloc",
+           "wl_column_product_noalloc", "wl_get_tuning", "wl_set_tuning", "wl_autotune",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
 PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
@@ -145,6 +167,11 @@ def load_library(path: str = LIB_PATH):
     L.wl_probe.restype = ctypes.c_int
     L.wl_column_product_noalloc.argtypes = [vp, ctypes.c_uint32, u64, u64, vp, ctypes.c_uint32, vp, vp]
     L.wl_column_product_noalloc.restype = ctypes.c_int
+    L.wl_get_tuning.argtypes = [vp, ctypes.POINTER(_Tuning)]
+    L.wl_set_tuning.argtypes = [vp, ctypes.POINTER(_Tuning)]
+    L.wl_autotune.argtypes = [vp, ctypes.POINTER(_Range), sz, u64, ctypes.c_uint32, ctypes.POINTER(_Tuning)]
+    for fn in ("wl_get_tuning", "wl_set_tuning", "wl_autotune"):
+        getattr(L, fn).restype = ctypes.c_int
     L.wl_server_open.argtypes = [ctypes.POINTER(_ServerOpts), ctypes.POINTER(vp)]
     L.wl_server_submit.argtypes = [vp, u64, u64, u64, ctypes.POINTER(u64)]
     L.wl_server_poll.argtypes = [vp, u64, ctypes.POINTER(_RequestInfo)]
@@ -273,6 +300,39 @@ class Engine:
         self._L.wl_drop_columns(self._ctx)
 
     @property
+    def tuning(self) -> dict:
+        t = _Tuning()
+        rc = self._L.wl_get_tuning(self._ctx, ctypes.byref(t))
+        if rc:
+            raise WilsonError(rc, "wl_get_tuning")
+        return t.to_dict()
+
+    @tuning.setter
+    def tuning(self, d: dict) -> None:
+        """Set some or all choices (keys of the `tuning` dict)."""
+        cur = self.tuning
+        cur.update(d)
+        t = _Tuning.from_dict(cur)
+        rc = self._L.wl_set_tuning(self._ctx, ctypes.byref(t))
+        if rc:
+            raise WilsonError(rc, "wl_set_tuning")
+
+    def autotune(self, ranges: Optional[Sequence[Tuple[int, int]]] = None, q_cap: int = 0, limbs=(2, 3, 4)) -> dict:
+        """Time the sweep kernel variants and keep the fastest in this context
+        (wl_autotune): on the given ranges (the workload), or on built-in
+        samples for the given limb widths."""
+        mask = 0
+        for L in limbs:
+            mask |= 1 << (L - 2)
+        t = _Tuning()
+        n = len(ranges) if ranges else 0
+        rr = (_Range * max(n, 1))(*[_Range(a, b) for a, b in (ranges or [])])
+        rc = self._L.wl_autotune(self._ctx, rr if n else None, n, q_cap, mask, ctypes.byref(t))
+        if rc:
+            raise WilsonError(rc, "wl_autotune")
+        return t.to_dict()
+
+    @property
     def stream(self) -> int:
         return self._L.wl_stream(self._ctx) or 0
 
@@ -369,10 +429,12 @@ class Server:
     column sweeps with the requests already running; each request's results
     equal those of ``Engine.search`` / ``Engine.rows`` on its range."""
 
-    def __init__(self, device: int = 0, pool_bytes: int = 0, step_cells: int = 0):
+    def __init__(self, device: int = 0, pool_bytes: int = 0, step_cells: int = 0, tuning: Optional[dict] = None):
         self._L = load_library()
         self._srv = ctypes.c_void_p()
-        o = _ServerOpts(device, 0, pool_bytes, step_cells)
+        self._tune = _Tuning.from_dict(tuning) if tuning else None
+        o = _ServerOpts(device, 0, pool_bytes, step_cells,
+                        ctypes.cast(ctypes.pointer(self._tune), ctypes.c_void_p) if tuning else None)
         rc = self._L.wl_server_open(ctypes.byref(o), ctypes.byref(self._srv))
         if rc:
             raise WilsonError(rc, "wl_server_open")

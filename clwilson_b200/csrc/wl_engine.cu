@@ -120,6 +120,7 @@ struct wl_ctx {
     int device = 0;
     int sms = 148;
     int cell_variant = 1;   // formulation of the sweep's cell step (see wl_kernels.cu cellv)
+    wl_tuning tune = {};     // sweep kernel choices per limb width (wl_autotune)
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;   // dense sweep, overlapped with the sparse sweep
     cudaEvent_t ev[8] = {};
@@ -141,6 +142,30 @@ struct wl_ctx {
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
 };
+
+// Sweep kernel choices measured best on B200 (the digit-sorted dense kernel
+// with 3-bit windows, H every 8 columns; the wide-product cell, two rows per
+// thread for large buckets; CTA-per-row merges from 64 splits).  The
+// environment overrides them for experiments: WL_CELL_VARIANT, WL_DENSE_SORT,
+// WL_DENSE_CFG (42: 4-bit windows), WL_DENSE_HSTEP; wl_autotune measures them.
+static void default_tuning(wl_ctx* c) {
+    const char* e;
+    int kernel = DENSE_SORTED_W3, hstep = 8;
+    const int sort = (e = getenv("WL_DENSE_SORT")) ? atoi(e) : 1;
+    const int cfg = (e = getenv("WL_DENSE_CFG")) ? atoi(e) : 0;
+    if ((e = getenv("WL_DENSE_HSTEP")) && atoi(e) > 0) hstep = atoi(e);
+    if (sort) kernel = cfg == 42 ? DENSE_SORTED_W4 : DENSE_SORTED_W3;
+    for (int L = 2; L <= 4; ++L) {
+        int k = kernel;
+        if (!sort) k = (cfg == 42 || (cfg == 0 && L != 4)) ? DENSE_SWITCH_W4 : DENSE_SWITCH_W3;
+        c->tune.sparse_variant[L - 2] = c->cell_variant;
+        c->tune.sparse_rpt[L - 2] = 2;
+        c->tune.dense_kernel[L - 2] = k;
+        c->tune.dense_hstep[L - 2] = hstep;
+        c->tune.ms[L - 2] = 0;
+    }
+    c->tune.merge_cta_min = 64;
+}
 
 // ---------------------------------------------------------------------------
 // column cache
@@ -362,7 +387,7 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
             ioff += g.items.size();
         }
         for (auto& g : lgroups) {
-            if (maxs >= 64)
+            if (maxs >= (uint32_t)c->tune.merge_cta_min)
                 launch_merge_cta(g.first, as<Bucket>(c->wbuckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
                                  as<uint4>(c->wpart), as<Deficit>(c->wdefs), g.second.first,
                                  g.second.second - g.second.first, as<uint4>(c->bacc), as<Deficit>(c->bdef), s3);
@@ -603,7 +628,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     // the partial-product budget
     auto plan_splits = [&](size_t i, double scale, uint64_t* Sd_out, uint64_t* Ss_out) {
         const uint32_t nrows_b = (uint32_t)hb[i].primes.size();
-        const int rpt = nrows_b >= 512 ? 2 : 1;
+        const int rpt = nrows_b >= 512 ? c->tune.sparse_rpt[hb[i].L - 2] : 1;
         const uint64_t nd = ndn[i], ns = ncol[i] - nd;
         uint64_t Sd = 0, Ss = 0;
         if (nd > 0) {
@@ -655,7 +680,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         b.type = h.type;
         b.range = h.range;
         int rpt, tps;
-        if (b.nrows >= 512) { rpt = 2; tps = 256; }
+        if (b.nrows >= 512) { rpt = c->tune.sparse_rpt[b.L - 2]; tps = 256; }
         else if (b.nrows >= 256) { rpt = 1; tps = 256; }
         else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
         const uint64_t nd = ndn[i];
@@ -848,9 +873,10 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         if (g.dense)
             launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint32_t>(c->dsplit),
-                               as<uint4>(c->part), as<Deficit>(c->defs), c->st2);
+                               as<uint4>(c->part), as<Deficit>(c->defs), c->st2, c->tune.dense_kernel[g.L - 2],
+                               (uint32_t)c->tune.dense_hstep[g.L - 2]);
         else
-            launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
+            launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
                          as<SweepItem>(c->items) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->cols),
                          as<uint4>(c->part), as<Deficit>(c->defs), c->st);
         if (!g.items.empty()) c->launches++;
@@ -868,7 +894,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             const int L = (int)db[ri[rb].bucket].L;
             uint32_t re = rb;
             while (re < nrows && (int)db[ri[re].bucket].L == L) ++re;
-            if (maxs >= 64)
+            if (maxs >= (uint32_t)c->tune.merge_cta_min)
                 launch_merge_cta(L, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
                                  as<uint4>(c->part), as<Deficit>(c->defs), rb, re - rb, as<uint4>(c->uacc),
                                  as<Deficit>(c->udef), c->st);
@@ -1065,6 +1091,7 @@ int wl_open(int device, wl_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return WL_ERR_CUDA; }
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* v = getenv("WL_CELL_VARIANT")) c->cell_variant = atoi(v);
+    default_tuning(c);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1187,6 +1214,128 @@ int wl_batch(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, wl_ran
     RunOut ro;
     RC(run_ranges(c, ranges, n, q_cap, ro, stats));
     return summarize(ro, n, q_cap == 0, out, results, cap, nresults, stats);
+}
+
+int wl_get_tuning(wl_ctx* c, wl_tuning* out) {
+    if (!c || !out) return WL_ERR_ARG;
+    *out = c->tune;
+    return 0;
+}
+
+int wl_set_tuning(wl_ctx* c, const wl_tuning* t) {
+    if (!c || !t) return WL_ERR_ARG;
+    for (int i = 0; i < 3; ++i) {
+        if (t->sparse_variant[i] < 0 || t->sparse_variant[i] > 2 || t->sparse_rpt[i] < 1 || t->sparse_rpt[i] > 2 ||
+            t->dense_kernel[i] < 0 || t->dense_kernel[i] > 3 || t->dense_hstep[i] < 1 || t->dense_hstep[i] > 4096)
+            return WL_ERR_ARG;
+    }
+    if (t->merge_cta_min < 1) return WL_ERR_ARG;
+    c->tune = *t;
+    return 0;
+}
+
+// One tuning measurement: the sweep-phase device time of the sample (best of
+// `reps` runs) and a digest of its rows, which every candidate must reproduce.
+static int tune_time(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, int reps, double* ms,
+                     uint64_t* digest) {
+    double best = 1e300;
+    for (int rep = 0; rep < reps; ++rep) {
+        RunOut ro;
+        wl_stats st;
+        RC(run_ranges(c, r, nr, qcap, ro, &st));
+        best = std::min(best, st.ms_sweep);
+        uint64_t d = 0;
+        for (const wl_row& w : ro.rows) d = d * 0x9E3779B97F4A7C15ull + (w.p ^ w.s0 ^ (w.s1 << 1) ^ (w.quot << 2));
+        *digest = d;
+    }
+    *ms = best;
+    return 0;
+}
+
+// Coordinate descent over the variants for the limb widths in `mask`, each
+// candidate applied to all of them, timed on ranges r[0..nr): the prefix-fold
+// sweep, then the dense sweep, then the merge fan-in.  A candidate replaces
+// the current choice only when it is more than 2% faster (run-to-run noise is
+// about 1%).
+static int tune_on(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, uint32_t mask, double* best_ms) {
+    uint64_t want = 0;
+    double ms;
+    uint64_t dg;
+    // calibration run (also the reference digest); one run per candidate when a run is long
+    RC(tune_time(c, r, nr, qcap, 1, &ms, &want));
+    const int reps = ms > 1000.0 ? 1 : 2;
+    RC(tune_time(c, r, nr, qcap, reps, &ms, &dg));
+    if (dg != want) return WL_ERR_CUDA;
+    double cur = ms;
+    auto apply = [&](auto f) { for (int L = 2; L <= 4; ++L) if (mask & (1u << (L - 2))) f(L - 2); };
+    auto trial = [&](const wl_tuning& t, bool* better) -> int {
+        const wl_tuning keep = c->tune;
+        c->tune = t;
+        RC(tune_time(c, r, nr, qcap, reps, &ms, &dg));
+        if (dg != want) {
+            fprintf(stderr, "wilson: autotune: kernel variants disagree\n");
+            c->tune = keep;
+            return WL_ERR_CUDA;
+        }
+        *better = ms < cur * 0.98;
+        if (*better) cur = ms;
+        else c->tune = keep;
+        return 0;
+    };
+    const int sparse_c[3][2] = { { 1, 1 }, { 0, 2 }, { 2, 2 } };   // (variant, rows per thread) besides (1, 2)
+    for (auto& sc : sparse_c) {
+        wl_tuning t = c->tune;
+        apply([&](int i) { t.sparse_variant[i] = sc[0]; t.sparse_rpt[i] = sc[1]; });
+        bool b;
+        RC(trial(t, &b));
+    }
+    const int dense_c[5][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 16 }, { DENSE_SORTED_W4, 8 },
+                                { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 } };
+    for (auto& dc : dense_c) {
+        wl_tuning t = c->tune;
+        apply([&](int i) { t.dense_kernel[i] = dc[0]; t.dense_hstep[i] = dc[1]; });
+        bool b;
+        RC(trial(t, &b));
+    }
+    for (int m : { 16, 256 }) {
+        wl_tuning t = c->tune;
+        t.merge_cta_min = m;
+        bool b;
+        RC(trial(t, &b));
+    }
+    *best_ms = cur;
+    return 0;
+}
+
+int wl_autotune(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, uint32_t limbs_mask, wl_tuning* out) {
+    if (!c || (n && !ranges)) return WL_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!limbs_mask) limbs_mask = 7;
+    if (n) {
+        // the caller's workload: one choice for all its limb widths
+        uint32_t mask = 0;
+        for (size_t k = 0; k < n; ++k) {
+            RC(wl_check_range(ranges[k].pmin, ranges[k].pmax));
+            mask |= 1u << (limb_width(ranges[k].pmax - 1) - 2);
+        }
+        double ms = 0;
+        RC(tune_on(c, ranges, n, q_cap, mask & limbs_mask, &ms));
+        for (int L = 2; L <= 4; ++L) if (mask & (1u << (L - 2))) c->tune.ms[L - 2] = ms;
+    } else {
+        // built-in samples, one per limb width, a mix of prefix-fold and dense columns
+        struct Sample { wl_range r; uint64_t qcap; };
+        const Sample smp[3] = { { { 1000000000ull, 1000300000ull }, 0 },
+                                { { 100000000000ull, 100000100000ull }, 1ull << 30 },
+                                { { (1ull << 62) - 100001ull, (1ull << 62) - 1ull }, 1ull << 27 } };
+        for (int L = 2; L <= 4; ++L) {
+            if (!(limbs_mask & (1u << (L - 2)))) continue;
+            double ms = 0;
+            RC(tune_on(c, &smp[L - 2].r, 1, smp[L - 2].qcap, 1u << (L - 2), &ms));
+            c->tune.ms[L - 2] = ms;
+        }
+    }
+    if (out) *out = c->tune;
+    return 0;
 }
 
 // parse_uint64 (putil.c:34-116): decimal/hex/octal with K,M,G,T,P (x1000),
@@ -1568,7 +1717,7 @@ static int serve_step(wl_server* s) {
         if (w.dense) {
             dense_shape(b.nrows, &rpt, &tps);
         } else {
-            if (b.nrows >= 512) rpt = 2;
+            if (b.nrows >= 512) rpt = c->tune.sparse_rpt[b.L - 2];
             if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
         }
         const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
@@ -1616,9 +1765,10 @@ static int serve_step(wl_server* s) {
         if (g.dense)
             launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(c->part),
-                               as<Deficit>(c->defs), c->st);
+                               as<Deficit>(c->defs), c->st,
+                               c->tune.dense_kernel[g.L - 2], (uint32_t)c->tune.dense_hstep[g.L - 2]);
         else
-            launch_sweep(c->cell_variant, g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
+            launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
                          as<SweepItem>(c->items) + ioff, as<RowMod>(s->mods), as<uint32_t>(c->cols),
                          as<uint4>(c->part), as<Deficit>(c->defs), c->st);
         s->ws.launches++;
@@ -1639,7 +1789,7 @@ static int serve_step(wl_server* s) {
             hi = std::max(hi, q->r0 + q->nrows);
         }
         if (!maxs) continue;
-        if (maxs >= 64)
+        if (maxs >= (uint32_t)c->tune.merge_cta_min)
             launch_merge_cta(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
                              as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
                              as<Deficit>(s->bdef), c->st);
@@ -1791,6 +1941,11 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
     wl_server* s = new wl_server();
     int rc = wl_open(o.device, &s->c);
     if (rc) { delete s; return rc; }
+    if (o.tuning && (rc = wl_set_tuning(s->c, o.tuning))) {
+        wl_close(s->c);
+        delete s;
+        return rc;
+    }
     s->pool_cap = (uint32_t)std::min<uint64_t>(bytes / WL_SERVER_ROW_BYTES, 1u << 30);
     s->step_cells = o.step_cells ? o.step_cells : (1ull << 32);
     s->bucket_cap = 3 * 1024;

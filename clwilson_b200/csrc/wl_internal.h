@@ -125,9 +125,12 @@ void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+// dense sweep kernels: digit-sorted windows (3-bit at 3 CTAs/SM, 4-bit at
+// 2 CTAs/SM) or a per-column bucket switch (same two shapes)
+enum { DENSE_SORTED_W3 = 0, DENSE_SORTED_W4 = 1, DENSE_SWITCH_W3 = 2, DENSE_SWITCH_W4 = 3 };
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
-                        cudaStream_t st);
+                        cudaStream_t st, int kernel, uint32_t hstep);
 void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t segs_per_cta, const uint32_t* base,
                       uint32_t nbase, uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
 void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,

@@ -1640,36 +1640,21 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
 }
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
-                        cudaStream_t st) {
+                        cudaStream_t st, int kernel, uint32_t hstep) {
     if (!nitems) return;
-    // tuning knobs (measured defaults): WL_DENSE_SORT (digit-sorted windows),
-    // WL_DENSE_HSTEP (columns per change of the high exponent part),
-    // WL_DENSE_CFG (window width and CTAs per SM of the unsorted kernel)
-    static const int env_sort = getenv("WL_DENSE_SORT") ? atoi(getenv("WL_DENSE_SORT")) : 1;
-    static const int env_hstep = getenv("WL_DENSE_HSTEP") ? atoi(getenv("WL_DENSE_HSTEP")) : 8;
-    static const int env_cfg = getenv("WL_DENSE_CFG") ? atoi(getenv("WL_DENSE_CFG")) : 0;
-    const uint32_t hstep = (uint32_t)(env_hstep > 0 ? env_hstep : 8);
+    if (hstep == 0) hstep = 8;
 #define WL_D(LL, MB, DWB, RR, SS) \
     k_sweep_dense<LL, MB, DWB, RR, SS><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs, hstep)
     if (rpt == 2) {
         if (L == 2) WL_D(2, 2, 3, 2, 0); else if (L == 3) WL_D(3, 2, 3, 2, 0); else WL_D(4, 2, 3, 2, 0);
-    } else if (env_sort) {
-        // digit-sorted windows: 3-bit windows at 3 CTAs/SM (WL_DENSE_CFG=42:
-        // 4-bit windows at 2 CTAs/SM)
-        if (env_cfg == 42) {
-            if (L == 2) WL_D(2, 2, 4, 1, 1); else if (L == 3) WL_D(3, 2, 4, 1, 1); else WL_D(4, 2, 4, 1, 1);
-        } else {
-            if (L == 2) WL_D(2, 3, 3, 1, 1); else if (L == 3) WL_D(3, 3, 3, 1, 1); else WL_D(4, 3, 3, 1, 1);
-        }
-    } else {
-        // 4-bit windows at 2 CTAs/SM for 2- and 3-limb residues, 3-bit windows
-        // at 3 CTAs/SM for 4-limb ones
-        const int cfg = env_cfg ? env_cfg : (L == 4 ? 33 : 42);
-        if (cfg == 33) {
-            if (L == 2) WL_D(2, 3, 3, 1, 0); else if (L == 3) WL_D(3, 3, 3, 1, 0); else WL_D(4, 3, 3, 1, 0);
-        } else {
-            if (L == 2) WL_D(2, 2, 4, 1, 0); else if (L == 3) WL_D(3, 2, 4, 1, 0); else WL_D(4, 2, 4, 1, 0);
-        }
+    } else if (kernel == DENSE_SORTED_W4) {
+        if (L == 2) WL_D(2, 2, 4, 1, 1); else if (L == 3) WL_D(3, 2, 4, 1, 1); else WL_D(4, 2, 4, 1, 1);
+    } else if (kernel == DENSE_SWITCH_W3) {
+        if (L == 2) WL_D(2, 3, 3, 1, 0); else if (L == 3) WL_D(3, 3, 3, 1, 0); else WL_D(4, 3, 3, 1, 0);
+    } else if (kernel == DENSE_SWITCH_W4) {
+        if (L == 2) WL_D(2, 2, 4, 1, 0); else if (L == 3) WL_D(3, 2, 4, 1, 0); else WL_D(4, 2, 4, 1, 0);
+    } else {   // DENSE_SORTED_W3
+        if (L == 2) WL_D(2, 3, 3, 1, 1); else if (L == 3) WL_D(3, 3, 3, 1, 1); else WL_D(4, 3, 3, 1, 1);
     }
 #undef WL_D
 }

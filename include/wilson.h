@@ -191,6 +191,36 @@ void wl_drop_columns(wl_ctx *ctx);
 int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p_bound, uint64_t T,
                               const uint32_t *cols, uint32_t ncols, uint64_t *s0s1, void *stream);
 
+/* ---- Kernel tuning ----------------------------------------------------------
+ * No counterpart in the reference.  The sweep kernels have variants whose
+ * speed depends on the GPU and the workload; a context keeps one choice per
+ * limb width L (index L - 2: p < 2^31, < 2^47, < 2^62). */
+#define WL_DENSE_SORTED_W3 0   /* digit-sorted windows, 3-bit, 3 CTAs/SM (default) */
+#define WL_DENSE_SORTED_W4 1   /* digit-sorted windows, 4-bit, 2 CTAs/SM */
+#define WL_DENSE_SWITCH_W3 2   /* per-column bucket switch, 3-bit, 3 CTAs/SM */
+#define WL_DENSE_SWITCH_W4 3   /* per-column bucket switch, 4-bit, 2 CTAs/SM */
+typedef struct {
+    int32_t sparse_variant[3];   /* cell formulation of the prefix-fold sweep: 0 carry chain, 1 wide products, 2 high half first */
+    int32_t sparse_rpt[3];       /* rows per thread of the prefix-fold sweep for buckets of >= 512 rows (1 or 2) */
+    int32_t dense_kernel[3];     /* WL_DENSE_* */
+    int32_t dense_hstep[3];      /* columns per change of the exponent's high part in the dense sweep */
+    int32_t merge_cta_min;       /* split count from which partials merge with one CTA per row (tree fan-in 256) */
+    int32_t pad;
+    double ms[3];                /* after wl_autotune: sweep time of the tuning sample per L (best choice) */
+} wl_tuning;
+
+int wl_get_tuning(wl_ctx *ctx, wl_tuning *out);
+int wl_set_tuning(wl_ctx *ctx, const wl_tuning *t);
+/* Time the variants and keep the fastest in the context, by coordinate
+ * descent (prefix-fold sweep, dense sweep, merge fan-in; a candidate must be
+ * more than 2% faster to replace the current choice).  ranges/n/q_cap: the
+ * workload to tune on (one choice for all its limb widths); n = 0: built-in
+ * samples, one per L with bit (L - 2) set in limbs_mask (0: all), a few
+ * seconds each.  Every candidate must produce the same rows; a mismatch
+ * returns WL_ERR_CUDA.  The choices are also written to *out when out != NULL. */
+int wl_autotune(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap, uint32_t limbs_mask,
+                wl_tuning *out);
+
 /* ---- Serving: a resident session with continuous batching ------------------
  *
  * No counterpart in the reference.  A server owns one GPU and a scheduler
@@ -216,6 +246,7 @@ typedef struct {
     uint32_t pad;
     uint64_t pool_bytes;   /* device memory for resident rows (0: 1 GiB); WL_SERVER_ROW_BYTES each */
     uint64_t step_cells;   /* column-cell budget of one scheduler step (0: 2^32) */
+    const wl_tuning *tuning;   /* kernel choices (NULL: the defaults) */
 } wl_server_opts;
 
 #define WL_SERVER_ROW_BYTES 160u

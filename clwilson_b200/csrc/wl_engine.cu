@@ -419,7 +419,7 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
 // the range's window (k_window_primes, k_compact); rs[i] gets the range's
 // window layout and its offset and count in tps.
 static int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<RangeState>& rs,
-                           std::vector<uint64_t>& tps) {
+                           std::vector<uint64_t>& tps, bool allow_empty = false) {
     rs.assign(nr, RangeState());
     uint64_t words = 0, segs = 0;
     for (size_t i = 0; i < nr; ++i) {
@@ -458,7 +458,7 @@ static int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::ve
             total += segcnt[r.seg_off + s];
         }
         r.ntp = total - r.tp_off;
-        if (r.ntp == 0) return WL_ERR_NOPRIMES;
+        if (r.ntp == 0 && !allow_empty) return WL_ERR_NOPRIMES;
     }
     offs[segs] = total;
     if (total >= (1ull << 31)) return WL_ERR_UNSUPPORTED;
@@ -1527,143 +1527,223 @@ static uint64_t class_target(uint64_t p, uint32_t* type) {
     return (p - 1) / 2;
 }
 
-// Admission: 0 admitted, 1 no room yet, < 0 the request fails with that code.
-static int serve_admit(wl_server* s, SReq* q) {
+// Admission of queued requests in FIFO order, all in one pass: one test-prime
+// pass over their ranges, one column-count query, the uploads while the stream
+// is idle, then every request's setup and tail launches and one synchronisation.
+// result[k]: 0 admitted, 1 no room yet (this and every later candidate stay
+// queued), < 0 the request fails with that code.
+static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std::vector<int>& result) {
     wl_ctx* c = s->c;
-    const bool full = q->qcap == 0;
+    const size_t nc = cands.size();
+    result.assign(nc, 1);
     cudaEventRecord(s->e0, c->st);
-    if (!q->have_tps) {
-        wl_range r = { q->pmin, q->pmax };
-        std::vector<RangeState> rs;
-        RC(gen_test_primes(c, &r, 1, rs, q->tps));
-        q->have_tps = true;
+    // 1. test primes of the candidates that have none yet
+    {
+        std::vector<size_t> need;
+        std::vector<wl_range> rr;
+        for (size_t k = 0; k < nc; ++k)
+            if (!cands[k]->have_tps) {
+                need.push_back(k);
+                rr.push_back({ cands[k]->pmin, cands[k]->pmax });
+            }
+        if (!need.empty()) {
+            std::vector<RangeState> rs;
+            std::vector<uint64_t> tps;
+            const int e = gen_test_primes(c, rr.data(), rr.size(), rs, tps, true);
+            s->ws.launches += 2 * rr.size();
+            for (size_t j = 0; j < need.size(); ++j) {
+                SReq* q = cands[need[j]];
+                if (e) { result[need[j]] = e; continue; }
+                q->tps.assign(tps.begin() + rs[j].tp_off, tps.begin() + rs[j].tp_off + rs[j].ntp);
+                q->have_tps = true;
+            }
+        }
     }
-    const uint32_t n = (uint32_t)q->tps.size();
-    if (n > s->pool_cap) return WL_ERR_NOMEM;
-    std::vector<uint64_t> byc[3];
-    uint64_t T[3] = { 0, 0, 0 };
-    for (uint64_t p : q->tps) {
-        uint32_t t;
-        const uint64_t Tp = class_target(p, &t);
-        if (byc[t].empty()) T[t] = Tp;
-        byc[t].push_back(p);
-    }
-    std::vector<int> kt;
-    std::vector<uint64_t> keys;
+    // 2. classes and targets; bucket slots and pool rows, first come first served
+    struct Adm {
+        SReq* q;
+        std::vector<uint64_t> byc[3];
+        uint64_t T[3];
+        std::vector<int> kt;
+        std::vector<uint64_t> keys;
+    };
+    std::vector<Adm> adm;
     uint64_t need = 0;
-    for (int t = 0; t < 3; ++t) {
-        if (byc[t].empty()) continue;
-        const uint64_t key = full ? T[t] : std::min(T[t], q->qcap - 1);
-        if (key >= (1ull << 32)) return WL_ERR_UNSUPPORTED;
-        kt.push_back(t);
-        keys.push_back(key);
-        need = std::max(need, key + 1);
+    for (size_t k = 0; k < nc; ++k) {
+        if (result[k] < 0) continue;
+        SReq* q = cands[k];
+        const bool full = q->qcap == 0;
+        const uint32_t n = (uint32_t)q->tps.size();
+        if (n == 0) { result[k] = WL_ERR_NOPRIMES; continue; }
+        if (n > s->pool_cap) { result[k] = WL_ERR_NOMEM; continue; }
+        Adm a;
+        a.q = q;
+        a.T[0] = a.T[1] = a.T[2] = 0;
+        for (uint64_t p : q->tps) {
+            uint32_t t;
+            const uint64_t Tp = class_target(p, &t);
+            if (a.byc[t].empty()) a.T[t] = Tp;
+            a.byc[t].push_back(p);
+        }
+        bool unsupported = false;
+        for (int t = 0; t < 3; ++t) {
+            if (a.byc[t].empty()) continue;
+            const uint64_t key = full ? a.T[t] : std::min(a.T[t], q->qcap - 1);
+            if (key >= (1ull << 32)) unsupported = true;
+            a.kt.push_back(t);
+            a.keys.push_back(key);
+        }
+        if (unsupported) { result[k] = WL_ERR_UNSUPPORTED; continue; }
+        uint32_t r0 = 0;
+        if (s->free_bids.size() < a.kt.size() || !pool_alloc(s, n, &r0)) break;
+        q->r0 = r0;
+        q->nrows = n;
+        q->L = limb_width(q->pmax - 1);
+        for (int t = 0; t < 3; ++t) q->targets[t] = a.T[t];
+        for (size_t i = 0; i < a.kt.size(); ++i) {
+            q->bids.push_back(*s->free_bids.begin());
+            s->free_bids.erase(s->free_bids.begin());
+            need = std::max(need, a.keys[i] + 1);
+        }
+        result[k] = 0;
+        adm.push_back(std::move(a));
     }
-    const size_t nk = kt.size();
-    if (s->free_bids.size() < nk) return 1;
-    uint32_t r0 = 0;
-    if (!pool_alloc(s, n, &r0)) return 1;
-    q->r0 = r0;
-    q->nrows = n;
-    q->L = limb_width(q->pmax - 1);
-    for (int t = 0; t < 3; ++t) q->targets[t] = T[t];
-    // column counts: columns <= key and dense columns (as the engine's step 3)
-    for (size_t i = 0; i < nk; ++i) {
-        const double Td = (double)T[kt[i]];
-        double qd = std::sqrt(Td) + 2;
-        for (int k = 0; k < 4; ++k) qd = std::sqrt(Td * std::log(std::max(qd, 3.0))) + 2;
-        keys.push_back(std::min<uint64_t>(qd >= 1.8e19 ? ~0ull : (uint64_t)qd, keys[i]));
-    }
+    if (adm.empty()) return;
+    auto fail_admitted = [&](int e) {
+        for (size_t k = 0; k < nc; ++k)
+            if (result[k] == 0) result[k] = e;
+    };
+    // 3. column counts of every admitted bucket (all columns, dense columns)
+    std::vector<uint64_t> keys;
+    for (auto& a : adm) keys.insert(keys.end(), a.keys.begin(), a.keys.end());
+    const size_t nk = keys.size();
+    for (auto& a : adm)
+        for (size_t i = 0; i < a.kt.size(); ++i) {
+            const double Td = (double)a.T[a.kt[i]];
+            double qd = std::sqrt(Td) + 2;
+            for (int k = 0; k < 4; ++k) qd = std::sqrt(Td * std::log(std::max(qd, 3.0))) + 2;
+            keys.push_back(std::min<uint64_t>(qd >= 1.8e19 ? ~0ull : (uint64_t)qd, a.keys[i]));
+        }
     int e = ensure_columns(c, need);
     if (!e) e = ensure(c->keys, keys.size() * 8);
     if (!e) e = ensure(c->counts, keys.size() * 8);
-    if (e) return e;
+    if (e) { fail_admitted(e); return; }
     std::vector<uint64_t> cnt(keys.size());
-    CK(cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st));
+    if (cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st) != cudaSuccess) {
+        fail_admitted(WL_ERR_CUDA);
+        return;
+    }
     launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->keys), (uint32_t)keys.size(),
                      as<uint64_t>(c->counts), c->st);
-    CK(cudaMemcpyAsync(cnt.data(), c->counts.p, keys.size() * 8, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
     s->ws.launches++;
-    // buckets and rows: by class, ascending p within a class
-    std::vector<RowInfo> ri(n);
-    uint32_t row = r0;
-    uint64_t Wt = 0;
-    for (size_t i = 0; i < nk; ++i) {
-        const int t = kt[i];
-        const uint32_t bid = *s->free_bids.begin();
-        s->free_bids.erase(s->free_bids.begin());
-        q->bids.push_back(bid);
-        SBucket& b = s->sb[bid];
-        b.used = true;
-        b.ncols = cnt[i];
-        b.cdense = std::min(cnt[nk + i], cnt[i]);
-        b.pos = 0;
-        b.nrows = (uint32_t)byc[t].size();
-        b.L = (uint32_t)q->L;
-        Bucket& d = s->pdesc[bid];
-        memset(&d, 0, sizeof(d));
-        d.T = T[t];
-        d.row_begin = row;
-        d.nrows = b.nrows;
-        d.L = b.L;
-        d.type = (uint32_t)t;
-        q->cells += (uint64_t)b.nrows * b.ncols;
-        for (uint64_t p : byc[t]) {
-            RowInfo& x = ri[row - r0];
-            uint32_t tt;
-            x.p = p;
-            x.Tp = class_target(p, &tt);
-            x.type = (uint32_t)t;
-            x.bucket = bid;
-            x.it_begin = 0;
-            x.it_count = 0;
-            if (full) Wt += x.Tp - d.T;
-            q->primes.push_back(p);
-            q->types.push_back((uint32_t)t);
-            ++row;
-        }
-        CK(cudaMemcpyAsync(as<Bucket>(s->pbuckets) + bid, &d, sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemsetAsync(as<Deficit>(s->bdef) + bid, 0, sizeof(Deficit), c->st));
+    if (cudaMemcpyAsync(cnt.data(), c->counts.p, keys.size() * 8, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+        cudaStreamSynchronize(c->st) != cudaSuccess) {
+        cudaGetLastError();
+        fail_admitted(WL_ERR_CUDA);
+        return;
     }
-    q->cells += Wt;
-    // the consecutive-integer tail (full searches): items of K integers
-    uint64_t K = 1, nitems = 0;
-    if (full && Wt) {
-        K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / ((double)c->sms * 2048.0 * 2.0)));
-        K = std::min<uint64_t>(K, 1u << 30);
-        for (uint32_t k = 0; k < n; ++k) {
-            const uint64_t len = ri[k].Tp - s->pdesc[ri[k].bucket].T;
-            ri[k].it_begin = (uint32_t)nitems;
-            ri[k].it_count = (uint32_t)((len + K - 1) / K);
-            nitems += ri[k].it_count;
+    // 4. buckets, rows and tail items on the host (tail items indexed globally
+    // in the admission's tail buffer)
+    std::vector<std::vector<RowInfo>> ris(adm.size());
+    std::vector<uint64_t> Ks(adm.size(), 1), item_off(adm.size(), 0), nitems(adm.size(), 0);
+    uint64_t items_total = 0;
+    size_t ki = 0;
+    for (size_t ai = 0; ai < adm.size(); ++ai) {
+        Adm& a = adm[ai];
+        SReq* q = a.q;
+        const bool full = q->qcap == 0;
+        std::vector<RowInfo>& ri = ris[ai];
+        ri.resize(q->nrows);
+        uint32_t row = q->r0;
+        uint64_t Wt = 0;
+        for (size_t i = 0; i < a.kt.size(); ++i, ++ki) {
+            const int t = a.kt[i];
+            const uint32_t bid = q->bids[i];
+            SBucket& b = s->sb[bid];
+            b.used = true;
+            b.ncols = cnt[ki];
+            b.cdense = std::min(cnt[nk + ki], cnt[ki]);
+            b.pos = 0;
+            b.nrows = (uint32_t)a.byc[t].size();
+            b.L = (uint32_t)q->L;
+            Bucket& d = s->pdesc[bid];
+            memset(&d, 0, sizeof(d));
+            d.T = a.T[t];
+            d.row_begin = row;
+            d.nrows = b.nrows;
+            d.L = b.L;
+            d.type = (uint32_t)t;
+            q->cells += (uint64_t)b.nrows * b.ncols;
+            for (uint64_t p : a.byc[t]) {
+                RowInfo& x = ri[row - q->r0];
+                uint32_t tt;
+                x.p = p;
+                x.Tp = class_target(p, &tt);
+                x.type = (uint32_t)t;
+                x.bucket = bid;
+                x.it_begin = 0;
+                x.it_count = 0;
+                if (full) Wt += x.Tp - d.T;
+                q->primes.push_back(p);
+                q->types.push_back((uint32_t)t);
+                ++row;
+            }
         }
-        if (nitems >= (1ull << 32)) return WL_ERR_UNSUPPORTED;
+        q->cells += Wt;
+        if (full && Wt) {
+            uint64_t K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / ((double)c->sms * 2048.0 * 2.0)));
+            K = std::min<uint64_t>(K, 1u << 30);
+            uint64_t ni = 0;
+            for (uint32_t k = 0; k < q->nrows; ++k) {
+                const uint64_t len = ri[k].Tp - s->pdesc[ri[k].bucket].T;
+                ri[k].it_begin = (uint32_t)(items_total + ni);
+                ri[k].it_count = (uint32_t)((len + K - 1) / K);
+                ni += ri[k].it_count;
+            }
+            Ks[ai] = K;
+            item_off[ai] = items_total;
+            nitems[ai] = ni;
+            items_total += ni;
+        }
     }
-    CK(cudaMemcpyAsync(as<RowInfo>(s->info) + r0, ri.data(), (size_t)n * sizeof(RowInfo), cudaMemcpyHostToDevice,
-                       c->st));
-    launch_setup_rows(as<RowInfo>(s->info) + r0, n, as<RowMod>(s->mods) + r0, c->st);
-    launch_acc_init(n, 0, as<uint4>(s->acc) + r0, nullptr, c->st);
-    s->ws.launches += 2;
-    if (nitems) {
-        RC(ensure(s->ipart, nitems * 16 + 16));
-        launch_iterate(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), r0, n, 0,
-                       (uint32_t)nitems, K, as<uint4>(s->ipart), c->st);
-        launch_tail_merge(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
-                          as<uint4>(s->ipart), K, r0, n, as<uint4>(s->acc), as<Deficit>(s->bdef), c->st);
+    if (items_total >= (1ull << 32)) { fail_admitted(WL_ERR_UNSUPPORTED); return; }
+    if (items_total && (e = ensure(s->ipart, items_total * 16 + 16))) { fail_admitted(e); return; }
+    // 5. uploads (the stream is idle), then the launches, one synchronisation
+    bool ok = true;
+    for (size_t ai = 0; ai < adm.size() && ok; ++ai) {
+        SReq* q = adm[ai].q;
+        ok &= cudaMemcpyAsync(as<RowInfo>(s->info) + q->r0, ris[ai].data(), (size_t)q->nrows * sizeof(RowInfo),
+                              cudaMemcpyHostToDevice, c->st) == cudaSuccess;
+        for (uint32_t bid : q->bids) {
+            ok &= cudaMemcpyAsync(as<Bucket>(s->pbuckets) + bid, &s->pdesc[bid], sizeof(Bucket),
+                                  cudaMemcpyHostToDevice, c->st) == cudaSuccess;
+            ok &= cudaMemsetAsync(as<Deficit>(s->bdef) + bid, 0, sizeof(Deficit), c->st) == cudaSuccess;
+        }
+    }
+    for (size_t ai = 0; ai < adm.size() && ok; ++ai) {
+        SReq* q = adm[ai].q;
+        launch_setup_rows(as<RowInfo>(s->info) + q->r0, q->nrows, as<RowMod>(s->mods) + q->r0, c->st);
+        launch_acc_init(q->nrows, 0, as<uint4>(s->acc) + q->r0, nullptr, c->st);
         s->ws.launches += 2;
-        // the tail is in the running product now: k_finish must not read it again
-        for (auto& x : ri) { x.it_begin = 0; x.it_count = 0; }
-        CK(cudaMemcpyAsync(as<RowInfo>(s->info) + r0, ri.data(), (size_t)n * sizeof(RowInfo),
-                           cudaMemcpyHostToDevice, c->st));
+        if (nitems[ai]) {
+            launch_iterate(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), q->r0, q->nrows,
+                           (uint32_t)item_off[ai], (uint32_t)nitems[ai], Ks[ai], as<uint4>(s->ipart), c->st);
+            launch_tail_merge(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                              as<uint4>(s->ipart), Ks[ai], q->r0, q->nrows, as<uint4>(s->acc), as<Deficit>(s->bdef),
+                              c->st);
+            launch_clear_tail(as<RowInfo>(s->info), q->r0, q->nrows, c->st);
+            s->ws.launches += 3;
+        }
     }
     cudaEventRecord(s->e1, c->st);
-    CK(cudaStreamSynchronize(c->st));
-    CK(cudaGetLastError());
+    if (!ok || cudaStreamSynchronize(c->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        cudaGetLastError();
+        fail_admitted(WL_ERR_CUDA);
+        return;
+    }
     float ms = 0;
     cudaEventElapsedTime(&ms, s->e0, s->e1);
     s->ws.ms_admit += ms;
-    return 0;
 }
 
 // One scheduler step: every bucket with columns left advances by one chunk.
@@ -1871,35 +1951,41 @@ static void serve_end(wl_server* s, SReq* q, int state, int rc) {
 static void serve_loop(wl_server* s) {
     cudaSetDevice(s->c->device);
     while (true) {
-        // admit queued requests in FIFO order while they fit
-        while (true) {
-            SReq* q = nullptr;
-            {
-                std::unique_lock<std::mutex> lk(s->mu);
-                while (!s->stop && s->queue.empty() && s->active.empty()) s->cv_work.wait(lk);
-                if (s->stop) return;
-                if (s->queue.empty()) break;
-                q = s->queue.front();
-                if (q->cancel) {
-                    s->queue.pop_front();
-                    serve_end(s, q, WL_REQ_CANCELLED, 0);
-                    continue;
+        // admit queued requests in FIFO order while they fit, all at once
+        std::vector<SReq*> cands;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (!s->stop && s->queue.empty() && s->active.empty()) s->cv_work.wait(lk);
+            if (s->stop) return;
+            for (auto it = s->queue.begin(); it != s->queue.end();) {
+                if ((*it)->cancel) {
+                    serve_end(s, *it, WL_REQ_CANCELLED, 0);
+                    it = s->queue.erase(it);
+                } else {
+                    cands.push_back(*it);
+                    ++it;
                 }
             }
-            const int r = serve_admit(s, q);
+        }
+        if (!cands.empty()) {
+            std::vector<int> res;
+            serve_admit_batch(s, cands, res);
             std::lock_guard<std::mutex> lk(s->mu);
-            if (r == 1 && !s->active.empty()) break;   // wait for rows to free up
-            s->queue.pop_front();
-            if (r) {
-                serve_release(s, q);
-                serve_end(s, q, WL_REQ_FAILED, r == 1 ? WL_ERR_NOMEM : r);
-                continue;
+            for (size_t k = 0; k < cands.size(); ++k) {
+                SReq* q = cands[k];
+                if (res[k] == 1) continue;                  // waits for rows to free up
+                s->queue.erase(std::find(s->queue.begin(), s->queue.end(), q));
+                if (res[k]) {
+                    serve_release(s, q);
+                    serve_end(s, q, WL_REQ_FAILED, res[k]);
+                    continue;
+                }
+                q->state = WL_REQ_ACTIVE;
+                q->t_admit = s->now_ms();
+                s->active.push_back(q);
+                q->tested = q->nrows;
+                s->ws.admitted++;
             }
-            q->state = WL_REQ_ACTIVE;
-            q->t_admit = s->now_ms();
-            s->active.push_back(q);
-            q->tested = q->nrows;
-            s->ws.admitted++;
             s->ws.peak_rows = std::max(s->ws.peak_rows, s->rows_used);
             s->ws.peak_active = std::max<uint32_t>(s->ws.peak_active, (uint32_t)s->active.size());
             s->stats = s->ws;

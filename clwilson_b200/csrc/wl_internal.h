@@ -148,6 +148,7 @@ void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMo
                   const Deficit* defs, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_acc_init(uint32_t nrows, uint32_t nbuckets, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_clear_below(uint32_t* bitmap, uint64_t lo, uint64_t q_lo, uint64_t nwords, cudaStream_t st);
+void launch_clear_tail(RowInfo* info, uint32_t row_begin, uint32_t nrows, cudaStream_t st);
 void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* ipart,
                        uint64_t K, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st);
 void launch_merge_cta(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,

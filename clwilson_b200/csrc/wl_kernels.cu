@@ -1720,6 +1720,21 @@ void launch_clear_below(uint32_t* bitmap, uint64_t lo, uint64_t q_lo, uint64_t n
     k_clear_below<<<(unsigned)((need + 255) / 256), 256, 0, st>>>(bitmap, lo, q_lo, need);
 }
 
+// The tail of rows [row_begin, row_begin + nrows) is in their running
+// products (k_tail_merge): k_finish must not multiply it in again.
+__global__ void k_clear_tail(RowInfo* __restrict__ info, uint32_t row_begin, uint32_t nrows) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nrows) {
+        info[row_begin + i].it_begin = 0;
+        info[row_begin + i].it_count = 0;
+    }
+}
+
+void launch_clear_tail(RowInfo* info, uint32_t row_begin, uint32_t nrows, cudaStream_t st) {
+    if (!nrows) return;
+    k_clear_tail<<<(nrows + 255) / 256, 256, 0, st>>>(info, row_begin, nrows);
+}
+
 void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* ipart,
                        uint64_t K, uint32_t row_begin, uint32_t nrows, uint4* acc, Deficit* bdef, cudaStream_t st) {
     if (!nrows) return;

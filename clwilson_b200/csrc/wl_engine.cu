@@ -147,7 +147,8 @@ struct wl_ctx {
 // with 3-bit windows, H every 8 columns; the wide-product cell, two rows per
 // thread for large buckets; CTA-per-row merges from 64 splits).  The
 // environment overrides them for experiments: WL_CELL_VARIANT, WL_DENSE_SORT,
-// WL_DENSE_CFG (42: 4-bit windows), WL_DENSE_HSTEP; wl_autotune measures them.
+// WL_DENSE_CFG (42: 4-bit windows), WL_DENSE_HSTEP, WL_DENSE_KERNEL (a
+// WL_DENSE_* value); wl_autotune measures them.
 static void default_tuning(wl_ctx* c) {
     const char* e;
     int kernel = DENSE_SORTED_W3, hstep = 8;
@@ -155,9 +156,11 @@ static void default_tuning(wl_ctx* c) {
     const int cfg = (e = getenv("WL_DENSE_CFG")) ? atoi(e) : 0;
     if ((e = getenv("WL_DENSE_HSTEP")) && atoi(e) > 0) hstep = atoi(e);
     if (sort) kernel = cfg == 42 ? DENSE_SORTED_W4 : DENSE_SORTED_W3;
+    const int forced = (e = getenv("WL_DENSE_KERNEL")) ? atoi(e) : -1;   // a WL_DENSE_* value
     for (int L = 2; L <= 4; ++L) {
         int k = kernel;
         if (!sort) k = (cfg == 42 || (cfg == 0 && L != 4)) ? DENSE_SWITCH_W4 : DENSE_SWITCH_W3;
+        if (forced >= 0 && forced <= DENSE_SMEM_W4) k = forced;
         c->tune.sparse_variant[L - 2] = c->cell_variant;
         c->tune.sparse_rpt[L - 2] = 2;
         c->tune.dense_kernel[L - 2] = k;
@@ -1226,7 +1229,7 @@ int wl_set_tuning(wl_ctx* c, const wl_tuning* t) {
     if (!c || !t) return WL_ERR_ARG;
     for (int i = 0; i < 3; ++i) {
         if (t->sparse_variant[i] < 0 || t->sparse_variant[i] > 2 || t->sparse_rpt[i] < 1 || t->sparse_rpt[i] > 2 ||
-            t->dense_kernel[i] < 0 || t->dense_kernel[i] > 3 || t->dense_hstep[i] < 1 || t->dense_hstep[i] > 4096)
+            t->dense_kernel[i] < 0 || t->dense_kernel[i] > 5 || t->dense_hstep[i] < 1 || t->dense_hstep[i] > 4096)
             return WL_ERR_ARG;
     }
     if (t->merge_cta_min < 1) return WL_ERR_ARG;
@@ -1289,8 +1292,9 @@ static int tune_on(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, uint3
         bool b;
         RC(trial(t, &b));
     }
-    const int dense_c[5][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 16 }, { DENSE_SORTED_W4, 8 },
-                                { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 } };
+    const int dense_c[7][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 16 }, { DENSE_SORTED_W4, 8 },
+                                { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 }, { DENSE_SMEM_W3, 8 },
+                                { DENSE_SMEM_W4, 8 } };
     for (auto& dc : dense_c) {
         wl_tuning t = c->tune;
         apply([&](int i) { t.dense_kernel[i] = dc[0]; t.dense_hstep[i] = dc[1]; });

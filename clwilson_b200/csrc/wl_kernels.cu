@@ -464,7 +464,11 @@ __device__ __forceinline__ void bucket_cell(Res<L> (&B)[RPT][NB], uint32_t d, ui
 // product when the run has two or more columns).
 constexpr uint32_t DENSE_GMAX = 32;   // splits per CTA at most (tps >= 8)
 
-template <int L, int MINB, int DW, int RPT, int SORT>
+// SMB = 1 (with SORT = 1, RPT = 1): the window buckets live in dynamic shared
+// memory (bucket d of thread t at sbk[d * 256 + t]); a digit's run loads its
+// bucket once, runs its cells in registers and stores it back.  That frees the
+// bucket registers (more CTAs per SM, or wider windows).
+template <int L, int MINB, int DW, int RPT, int SORT, int SMB = 0>
 __global__ void __launch_bounds__(256, MINB)
 k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
               const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, const uint32_t* __restrict__ dsplit,
@@ -475,6 +479,8 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     constexpr int NBK = (1 << DW) - 1;          // buckets per window
     __shared__ uint32_t scnt[DENSE_GMAX][NBK + 1];        // deficit of bucket d, in units of 32 bits
     __shared__ uint32_t scur[SORT ? DENSE_GMAX : 1][NBK + 1];
+    extern __shared__ uint4 sbk[];                         // SMB: NBK x 256 buckets
+    static_assert(!SMB || (SORT && RPT == 1), "shared-memory buckets need the sorted kernel, one row per thread");
     const SweepItem it = items[blockIdx.x];
     const Bucket bk = buckets[it.bucket];
     const uint32_t tps = it.tps;
@@ -582,11 +588,16 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     for (int j = 0; j < RPT; ++j) set_small<L>(acc[j], 1);
     u128 defacc = 0;
     for (int w = (int)nwin - 1; w >= 0; --w) {
-        Res<L> B[RPT][NBK];
+        Res<L> B[SMB ? 1 : RPT][SMB ? 1 : NBK];
+        if (SMB) {
 #pragma unroll
-        for (int j = 0; j < RPT; ++j)
+            for (int d = 0; d < NBK; ++d) sbk[d * 256 + threadIdx.x] = make_uint4(1, 0, 0, 0);
+        } else {
 #pragma unroll
-            for (int d = 0; d < NBK; ++d) set_small<L>(B[j][d], 1);
+            for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                for (int d = 0; d < NBK; ++d) set_small<L>(B[j][d], 1);
+        }
         __syncthreads();
         for (uint32_t k = lt; k <= NBK; k += tps) scnt[g][k] = 0;
         for (uint32_t ch = 0; ch < nchunks; ++ch) {
@@ -632,14 +643,22 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
 #pragma unroll
                 for (int d = 1; d <= NBK; ++d) {
                     const uint32_t k0 = scur[g][d - 1], k1 = scur[g][d];
+                    if (SMB) {
+                        if (k1 == k0) continue;
+                        const uint4 v = sbk[(d - 1) * 256 + threadIdx.x];
+                        Res<L>& b = B[0][0];
+                        b.w[0] = v.x; b.w[1] = v.y;
+                        if (L > 2) b.w[2 < L ? 2 : 0] = v.z;
+                        if (L > 3) b.w[3 < L ? 3 : 0] = v.w;
+                    }
                     uint32_t k = k0;
                     for (; k + 1 < k1; k += 2) {
                         const uint32_t qa = ss[base + k], qb = ss[base + k + 1];
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) {
-                            cell_w<L>(B[j][d - 1], qa, n[j], ninv[j]);
+                            cell_w<L>(B[j][SMB ? 0 : d - 1], qa, n[j], ninv[j]);
                             cell_w<L>(X[j], qb, n[j], ninv[j]);
-                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][d - 1], n[j]);
+                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][SMB ? 0 : d - 1], n[j]);
                             if (L != 2 && qb >= 0x80000000u) cond_sub_chain(X[j], n[j]);
                         }
                     }
@@ -647,23 +666,30 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
                         const uint32_t qa = ss[base + k];
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) {
-                            cell_w<L>(B[j][d - 1], qa, n[j], ninv[j]);
-                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][d - 1], n[j]);
+                            cell_w<L>(B[j][SMB ? 0 : d - 1], qa, n[j], ninv[j]);
+                            if (L != 2 && qa >= 0x80000000u) cond_sub_chain(B[j][SMB ? 0 : d - 1], n[j]);
                         }
                     }
                     if (k1 - k0 >= 2) {
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) {
-                            B[j][d - 1] = mont_mul<L>(B[j][d - 1], X[j], n[j], ninv[j]);
+                            B[j][SMB ? 0 : d - 1] = mont_mul<L>(B[j][SMB ? 0 : d - 1], X[j], n[j], ninv[j]);
                             set_small<L>(X[j], 1);
                         }
+                    }
+                    if (SMB) {
+                        const Res<L>& b = B[0][0];
+                        sbk[(d - 1) * 256 + threadIdx.x] =
+                            make_uint4(b.w[0], b.w[1], L > 2 ? b.w[2 < L ? 2 : 0] : 0, L > 3 ? b.w[3 < L ? 3 : 0] : 0);
                     }
                 }
             } else {
                 for (uint32_t k = 0; k < nh; ++k) {
                     const uint32_t d = (uint32_t)sm[base + k];
                     const uint32_t q = sq[base + k];
-                    if (d) bucket_cell<L, NBK, RPT>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
+                    if constexpr (!SMB) {
+                        if (d) bucket_cell<L, NBK, RPT>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
+                    }
                 }
             }
         }
@@ -677,10 +703,19 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
         }
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
-            Res<L> S = B[j][NBK - 1], R = B[j][NBK - 1];
+            auto bucket = [&](int d) -> Res<L> {
+                if (!SMB) return B[j][SMB ? 0 : d];
+                const uint4 v = sbk[d * 256 + threadIdx.x];
+                Res<L> b;
+                b.w[0] = v.x; b.w[1] = v.y;
+                if (L > 2) b.w[2 < L ? 2 : 0] = v.z;
+                if (L > 3) b.w[3 < L ? 3 : 0] = v.w;
+                return b;
+            };
+            Res<L> S = bucket(NBK - 1), R = S;
 #pragma unroll
             for (int d = NBK - 2; d >= 0; --d) {
-                S = mont_mul<L>(S, B[j][d], n[j], ninv[j]);
+                S = mont_mul<L>(S, bucket(d), n[j], ninv[j]);
                 R = mont_mul<L>(R, S, n[j], ninv[j]);
             }
             if (w == (int)nwin - 1) {
@@ -1645,8 +1680,24 @@ void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, 
     if (hstep == 0) hstep = 8;
 #define WL_D(LL, MB, DWB, RR, SS) \
     k_sweep_dense<LL, MB, DWB, RR, SS><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs, hstep)
+#define WL_DS(LL, MB, DWB) do {                                                                   \
+        constexpr int nbk_ = (1 << DWB) - 1;                                                           \
+        const int smem_ = nbk_ * 256 * (int)sizeof(uint4);                                             \
+        static bool attr_ = false;                                                                      \
+        if (!attr_) {                                                                                   \
+            cudaFuncSetAttribute(k_sweep_dense<LL, MB, DWB, 1, 1, 1>,                                   \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);                   \
+            attr_ = true;                                                                               \
+        }                                                                                               \
+        k_sweep_dense<LL, MB, DWB, 1, 1, 1><<<nitems, 256, smem_, st>>>(buckets, items, mods, cols, dsplit, \
+                                                                      part, defs, hstep);               \
+    } while (0)
     if (rpt == 2) {
         if (L == 2) WL_D(2, 2, 3, 2, 0); else if (L == 3) WL_D(3, 2, 3, 2, 0); else WL_D(4, 2, 3, 2, 0);
+    } else if (kernel == DENSE_SMEM_W3) {
+        if (L == 2) WL_DS(2, 4, 3); else if (L == 3) WL_DS(3, 4, 3); else WL_DS(4, 4, 3);
+    } else if (kernel == DENSE_SMEM_W4) {
+        if (L == 2) WL_DS(2, 2, 4); else if (L == 3) WL_DS(3, 2, 4); else WL_DS(4, 2, 4);
     } else if (kernel == DENSE_SORTED_W4) {
         if (L == 2) WL_D(2, 2, 4, 1, 1); else if (L == 3) WL_D(3, 2, 4, 1, 1); else WL_D(4, 2, 4, 1, 1);
     } else if (kernel == DENSE_SWITCH_W3) {
@@ -1657,6 +1708,7 @@ void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, 
         if (L == 2) WL_D(2, 3, 3, 1, 1); else if (L == 3) WL_D(3, 3, 3, 1, 1); else WL_D(4, 3, 3, 1, 1);
     }
 #undef WL_D
+#undef WL_DS
 }
 void launch_iterate(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, uint32_t row_begin,
                     uint32_t nrows, uint32_t item_begin, uint32_t nitems, uint64_t K, uint4* out, cudaStream_t st) {

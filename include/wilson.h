@@ -199,6 +199,8 @@ int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p
 #define WL_DENSE_SORTED_W4 1   /* digit-sorted windows, 4-bit, 2 CTAs/SM */
 #define WL_DENSE_SWITCH_W3 2   /* per-column bucket switch, 3-bit, 3 CTAs/SM */
 #define WL_DENSE_SWITCH_W4 3   /* per-column bucket switch, 4-bit, 2 CTAs/SM */
+#define WL_DENSE_SMEM_W3   4   /* digit-sorted, buckets in shared memory, 3-bit, 4 CTAs/SM */
+#define WL_DENSE_SMEM_W4   5   /* digit-sorted, buckets in shared memory, 4-bit, 2 CTAs/SM */
 typedef struct {
     int32_t sparse_variant[3];   /* cell formulation of the prefix-fold sweep: 0 carry chain, 1 wide products, 2 high half first */
     int32_t sparse_rpt[3];       /* rows per thread of the prefix-fold sweep for buckets of >= 512 rows (1 or 2) */

@@ -110,7 +110,8 @@ def test_capped_golden(engine, golden, lo, hi, qcap):
         assert st.targets[int(t)] == T
 
 
-@pytest.mark.parametrize("lo,hi", [(10**13, 10**13 + 20000), ((1 << 62) - 1 - 20000, (1 << 62) - 1)])
+@pytest.mark.parametrize("lo,hi", [(10**13, 10**13 + 20000), ((1 << 62) - 1 - 20000, (1 << 62) - 1),
+                                   ((1 << 47) - 2000, (1 << 47) + 2000)])   # 3 -> 4 limbs across the range
 def test_capped_parity_with_oracle(engine, lo, hi):
     qcap = 1 << 20
     got, _ = engine.rows(lo, hi, q_cap=qcap)

@@ -38,7 +38,7 @@ def _capped_ok(e, golden, lo, hi, qcap):
         assert (int(r["s0"]), int(r["s1"])) == (w["s0"], w["s1"]), w["p"]
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("hstep", [4, 16])
 def test_dense_variants(eng, golden, kernel, hstep):
     eng.tuning = {"dense_kernel": [kernel] * 3, "dense_hstep": [hstep] * 3}

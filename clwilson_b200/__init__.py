@@ -124,7 +124,8 @@ SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", 
            "wl_column_product_noalloc", "wl_get_tuning", "wl_set_tuning", "wl_autotune",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
-PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4}
+PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5, "dfma": 6, "mad+dfma": 7,
+          "madwide+dfma": 8}
 
 _lib = None
 

@@ -5,6 +5,10 @@
 //   WL_PROBE_MADHI   mad.hi.u32, 8 independent chains per thread
 //   WL_PROBE_CELL2/3/4  the sweep's cell step (wl_arith.cuh) at L = 2, 3, 4,
 //                    4 independent rows per thread, operands in registers
+//   WL_PROBE_DFMA    fma.rn.f64, 8 independent chains per thread
+//   WL_PROBE_MAD_DFMA / WL_PROBE_MADWIDE_DFMA  mad.lo.u32 (or mad.wide.u32) and
+//                    fma.rn.f64 chains interleaved, both counted: whether the
+//                    FP64 pipe adds multiply throughput next to the integer one
 //
 // Each result is operations (or cells) per second over the whole GPU, timed
 // with CUDA events around one launch sized to run for tens of milliseconds.
@@ -76,6 +80,40 @@ __global__ void __launch_bounds__(256) k_probe_madwide(uint32_t iters, uint32_t 
     out[blockIdx.x * blockDim.x + threadIdx.x] = x;
 }
 
+// MODE 0: fma.rn.f64 only; 1: mad.lo.u32 + fma.rn.f64; 2: mad.wide.u32 + fma.rn.f64
+template <int MODE>
+__global__ void __launch_bounds__(256) k_probe_dfma(uint32_t iters, uint32_t seed, uint32_t* out) {
+    double d[8];
+    uint32_t a[8];
+    uint64_t w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        d[k] = 1.0 + (double)(threadIdx.x + k) * 1e-3;
+        a[k] = seed + threadIdx.x * 8 + k;
+        w[k] = a[k];
+    }
+    const double dm = 0.9999999, dc = 1e-3;
+    const uint32_t m = 0x9E3779B1u ^ seed, c = 0x7F4A7C15u;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(d[k]) : "d"(dm), "d"(dc));
+                if (MODE == 1) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
+                if (MODE == 2) {
+                    uint32_t lo = (uint32_t)w[k];
+                    asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[k]) : "r"(lo), "r"(m));
+                }
+            }
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x ^= (uint32_t)__double2uint_rz(d[k]) ^ a[k] ^ (uint32_t)w[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+}
+
 template <int L, int V>
 __global__ void __launch_bounds__(256) k_probe_cell(uint32_t iters, uint32_t seed, uint32_t* out) {
     // a fixed odd modulus n < 2^(32L-2) and its -n^-1 mod 2^32
@@ -136,6 +174,9 @@ extern "C" int wl_probe(int device, int which, double* rate) {
             case WL_PROBE_CELL3: k_probe_cell<3, WL_CELL_VARIANT><<<blocks, threads>>>(it, 12345u, out); break;
             case WL_PROBE_CELL4: k_probe_cell<4, WL_CELL_VARIANT><<<blocks, threads>>>(it, 12345u, out); break;
             case WL_PROBE_MADWIDE: k_probe_madwide<<<blocks, threads>>>(it, 12345u, out); break;
+            case WL_PROBE_DFMA: k_probe_dfma<0><<<blocks, threads>>>(it, 12345u, out); break;
+            case WL_PROBE_MAD_DFMA: k_probe_dfma<1><<<blocks, threads>>>(it, 12345u, out); break;
+            case WL_PROBE_MADWIDE_DFMA: k_probe_dfma<2><<<blocks, threads>>>(it, 12345u, out); break;
             case 100: k_probe_cell<2, 0><<<blocks, threads>>>(it, 12345u, out); break;
             case 101: k_probe_cell<2, 1><<<blocks, threads>>>(it, 12345u, out); break;
             case 102: k_probe_cell<2, 2><<<blocks, threads>>>(it, 12345u, out); break;
@@ -147,7 +188,13 @@ extern "C" int wl_probe(int device, int which, double* rate) {
             default: k_probe_cell<4, 2><<<blocks, threads>>>(it, 12345u, out); break;
         }
     };
-    if (which == WL_PROBE_MAD || which == WL_PROBE_MADHI || which == WL_PROBE_MADWIDE) { per_iter = 32; iters = 200000; }
+    if (which == WL_PROBE_MAD || which == WL_PROBE_MADHI || which == WL_PROBE_MADWIDE || which == WL_PROBE_DFMA) {
+        per_iter = 32;
+        iters = 200000;
+    } else if (which == WL_PROBE_MAD_DFMA || which == WL_PROBE_MADWIDE_DFMA) {
+        per_iter = 64;   // both kinds of operation
+        iters = 100000;
+    }
     else if ((which >= WL_PROBE_CELL2 && which <= WL_PROBE_CELL4) || (which >= 100 && which <= 122)) {
         per_iter = 16; iters = 20000;
     }

@@ -1,0 +1,102 @@
+// wl_host.h -- host-side internals shared by the engine (wl_engine.cu) and the
+// serving session (wl_serve.cu): device buffers, error macros, the context.
+#pragma once
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "wilson.h"
+#include "wl_internal.h"
+
+// A growable device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+inline int ensure(DevBuf& b, size_t bytes) {
+    if (bytes <= b.cap && b.p) return 0;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t nb = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&b.p, nb) != cudaSuccess) {
+        cudaGetLastError();
+        return WL_ERR_NOMEM;
+    }
+    b.cap = nb;
+    return 0;
+}
+
+template <class T> inline T* as(DevBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+// Limb width of residues mod p^2 for primes up to pmax_incl.
+inline int limb_width(uint64_t pmax_incl) {
+    if (pmax_incl < (1ull << 31)) return 2;
+    if (pmax_incl < (1ull << 47)) return 3;
+    return 4;
+}
+
+#define CK(x)                                                        \
+    do {                                                             \
+        cudaError_t e_ = (x);                                        \
+        if (e_ != cudaSuccess) {                                     \
+            fprintf(stderr, "wilson: CUDA error %s at %s:%d\n",      \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return WL_ERR_CUDA;                                      \
+        }                                                            \
+    } while (0)
+
+#define RC(x)                      \
+    do {                           \
+        int r_ = (x);              \
+        if (r_) return r_;         \
+    } while (0)
+
+struct wl_ctx {
+    int device = 0;
+    int sms = 148;
+    int cell_variant = 1;   // formulation of the sweep's cell step (see wl_kernels.cu cellv)
+    wl_tuning tune = {};     // sweep kernel choices per limb width (wl_autotune)
+    cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;   // dense sweep, overlapped with the sparse sweep
+    cudaEvent_t ev[8] = {};
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t big0 = nullptr, big1 = nullptr;
+    cudaEvent_t rows_ready = nullptr;   // row tables uploaded and k_setup_rows done (main stream)
+    double ms_big = 0;
+    DevBuf base;            // odd primes < 65536 (sieving primes of the column sieve)
+    uint32_t nbase = 0;
+    DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
+    uint64_t ncols = 0, col_limit = 0;
+    DevBuf bitmap, segcount, offsets;
+    DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout, dsplit;
+    // columns above 2^32
+    cudaStream_t st3 = nullptr;
+    DevBuf bbitmap, bsegcount, boffsets, boffs, wcols, wbuckets, witems, wpart, wdefs, bacc, bdef, wkeys, wcounts;
+    DevBuf uacc, udef;   // columns below 2^32: per-row product of all splits, per-bucket deficit
+    uint32_t launches = 0;
+    uint64_t h2d = 0, d2h = 0;
+    double ms_sieve = 0;
+};
+
+// A range's window of test primes and its classes.
+struct RangeState {
+    uint64_t pmin, pmax, lo0;
+    uint32_t nseg;
+    uint64_t word_off, seg_off;
+    uint64_t tp_off = 0, ntp = 0;
+    uint64_t T[3] = { 0, 0, 0 };
+    uint64_t per_class[3] = { 0, 0, 0 };
+};
+
+// Every prime below `limit` (<= 2^32) in the context's resident column table.
+int ensure_columns(wl_ctx* c, uint64_t limit);
+// Test primes of each range, ascending (deterministic Miller-Rabin on the
+// device); with allow_empty a range without primes is not an error.
+int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<RangeState>& rs,
+                    std::vector<uint64_t>& tps, bool allow_empty = false);
+// results.txt value of one row (cl_wilson.cpp:872-898): 1 if it is a result line.
+int result_of(const wl_row& r, int32_t* value);

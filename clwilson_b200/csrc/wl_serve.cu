@@ -1,0 +1,806 @@
+// wl_serve.cu -- serving sessions of the Wilson-prime engine (wl_server_*).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <set>
+#include <thread>
+#include <vector>
+
+#include "wilson.h"
+#include "wl_internal.h"
+#include "wl_host.h"
+
+using namespace wl;
+
+// ===========================================================================
+// Serving: a resident session with continuous batching (wl_server_*).
+//
+// The rows of every admitted request live in a device row pool (RowInfo,
+// RowMod, a running product per row, RowOut); their (request, class) buckets
+// hold a slot of the bucket table (persistent descriptor plus the bucket's
+// accumulated power-of-two deficit).  One scheduler thread owns the GPU:
+//   admit   queued requests in FIFO order while the pool has room: test
+//           primes, classes and targets, column counts, moduli, and for a full
+//           search the consecutive-integer tail folded into each row's running
+//           product (k_iterate + k_tail_merge);
+//   step    every admitted bucket advances by one chunk of its columns (an
+//           equal share of the step's cell budget): the engine's sweep kernels
+//           over [pos, pos + len) -- through Bucket::cbase -- in one launch per
+//           (limb width, sweep kind) for all buckets, then k_merge* folds the
+//           chunk's split products into the resident running products;
+//   finish  requests whose buckets reached their last column: k_finish in
+//           merged mode over the request's rows, result lines and checksum
+//           (cl_wilson.cpp:872-900); the rows and slots are freed.
+// ===========================================================================
+
+namespace {
+
+struct SBucket {
+    bool used = false;
+    uint64_t ncols = 0, cdense = 0, pos = 0;   // columns [0, ncols), dense [0, cdense), next column
+    uint32_t nrows = 0, L = 2;
+};
+
+struct SReq {
+    uint64_t id = 0, pmin = 0, pmax = 0, qcap = 0;
+    int state = WL_REQ_QUEUED, rc = 0;
+    bool cancel = false;
+    bool have_tps = false;
+    std::vector<uint64_t> tps;        // test primes, ascending
+    uint32_t r0 = 0, nrows = 0;
+    int L = 2;
+    std::vector<uint32_t> bids;
+    std::vector<uint64_t> primes;     // pool order: row r0 + k holds primes[k]
+    std::vector<uint32_t> types;
+    uint64_t targets[3] = { 0, 0, 0 };
+    uint64_t checksum = 0, cells = 0;
+    uint64_t tested = 0;              // set under the server's mutex
+    std::vector<wl_row> rows;         // ascending p, once done
+    std::vector<wl_result> lines;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+};
+
+}  // namespace
+
+struct wl_server {
+    wl_ctx* c = nullptr;
+    uint32_t pool_cap = 0, bucket_cap = 0;
+    uint64_t step_cells = 0;
+    DevBuf info, mods, acc, out, pbuckets, sbuckets, bdef, ipart;
+    std::vector<SBucket> sb;
+    std::vector<Bucket> pdesc;                 // persistent descriptors (device copy: pbuckets)
+    std::map<uint32_t, uint32_t> free_rows;    // first row -> length
+    std::set<uint32_t> free_bids;
+    uint32_t rows_used = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<SReq*> queue;
+    std::map<uint64_t, SReq*> reqs;
+    std::vector<SReq*> active;                 // scheduler thread only
+    std::thread worker;
+    bool stop = false;
+    uint64_t next_id = 1;
+    wl_server_stats stats = {};    // published copy (under mu)
+    wl_server_stats ws = {};       // scheduler thread's own
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+static bool pool_alloc(wl_server* s, uint32_t n, uint32_t* r0) {
+    for (auto it = s->free_rows.begin(); it != s->free_rows.end(); ++it) {
+        if (it->second < n) continue;
+        *r0 = it->first;
+        const uint32_t rest = it->second - n, start = it->first + n;
+        s->free_rows.erase(it);
+        if (rest) s->free_rows[start] = rest;
+        s->rows_used += n;
+        return true;
+    }
+    return false;
+}
+
+static void pool_free(wl_server* s, uint32_t r0, uint32_t n) {
+    s->rows_used -= n;
+    auto it = s->free_rows.emplace(r0, n).first;
+    auto nx = std::next(it);
+    if (nx != s->free_rows.end() && it->first + it->second == nx->first) {
+        it->second += nx->second;
+        s->free_rows.erase(nx);
+    }
+    if (it != s->free_rows.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) {
+            pv->second += it->second;
+            s->free_rows.erase(it);
+        }
+    }
+}
+
+static void serve_release(wl_server* s, SReq* q) {
+    for (uint32_t bid : q->bids) {
+        s->sb[bid] = SBucket();
+        memset(&s->pdesc[bid], 0, sizeof(Bucket));
+        s->free_bids.insert(bid);
+    }
+    q->bids.clear();
+    if (q->nrows) pool_free(s, q->r0, q->nrows);
+    q->nrows = 0;
+}
+
+static uint64_t class_target(uint64_t p, uint32_t* type) {
+    if (p % 3 == 1) { *type = 0; return (p - 1) / 6; }
+    if (p % 12 == 5) { *type = 1; return (p - 1) / 4; }
+    *type = 2;
+    return (p - 1) / 2;
+}
+
+// Admission of queued requests in FIFO order, all in one pass: one test-prime
+// pass over their ranges, one column-count query, the uploads while the stream
+// is idle, then every request's setup and tail launches and one synchronisation.
+// result[k]: 0 admitted, 1 no room yet (this and every later candidate stay
+// queued), < 0 the request fails with that code.
+static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std::vector<int>& result) {
+    wl_ctx* c = s->c;
+    const size_t nc = cands.size();
+    result.assign(nc, 1);
+    cudaEventRecord(s->e0, c->st);
+    // 1. test primes of the candidates that have none yet
+    {
+        std::vector<size_t> need;
+        std::vector<wl_range> rr;
+        for (size_t k = 0; k < nc; ++k)
+            if (!cands[k]->have_tps) {
+                need.push_back(k);
+                rr.push_back({ cands[k]->pmin, cands[k]->pmax });
+            }
+        if (!need.empty()) {
+            std::vector<RangeState> rs;
+            std::vector<uint64_t> tps;
+            const int e = gen_test_primes(c, rr.data(), rr.size(), rs, tps, true);
+            s->ws.launches += 2 * rr.size();
+            for (size_t j = 0; j < need.size(); ++j) {
+                SReq* q = cands[need[j]];
+                if (e) { result[need[j]] = e; continue; }
+                q->tps.assign(tps.begin() + rs[j].tp_off, tps.begin() + rs[j].tp_off + rs[j].ntp);
+                q->have_tps = true;
+            }
+        }
+    }
+    // 2. classes and targets; bucket slots and pool rows, first come first served
+    struct Adm {
+        SReq* q;
+        std::vector<uint64_t> byc[3];
+        uint64_t T[3];
+        std::vector<int> kt;
+        std::vector<uint64_t> keys;
+    };
+    std::vector<Adm> adm;
+    uint64_t need = 0;
+    for (size_t k = 0; k < nc; ++k) {
+        if (result[k] < 0) continue;
+        SReq* q = cands[k];
+        const bool full = q->qcap == 0;
+        const uint32_t n = (uint32_t)q->tps.size();
+        if (n == 0) { result[k] = WL_ERR_NOPRIMES; continue; }
+        if (n > s->pool_cap) { result[k] = WL_ERR_NOMEM; continue; }
+        Adm a;
+        a.q = q;
+        a.T[0] = a.T[1] = a.T[2] = 0;
+        for (uint64_t p : q->tps) {
+            uint32_t t;
+            const uint64_t Tp = class_target(p, &t);
+            if (a.byc[t].empty()) a.T[t] = Tp;
+            a.byc[t].push_back(p);
+        }
+        bool unsupported = false;
+        for (int t = 0; t < 3; ++t) {
+            if (a.byc[t].empty()) continue;
+            const uint64_t key = full ? a.T[t] : std::min(a.T[t], q->qcap - 1);
+            if (key >= (1ull << 32)) unsupported = true;
+            a.kt.push_back(t);
+            a.keys.push_back(key);
+        }
+        if (unsupported) { result[k] = WL_ERR_UNSUPPORTED; continue; }
+        uint32_t r0 = 0;
+        if (s->free_bids.size() < a.kt.size() || !pool_alloc(s, n, &r0)) break;
+        q->r0 = r0;
+        q->nrows = n;
+        q->L = limb_width(q->pmax - 1);
+        for (int t = 0; t < 3; ++t) q->targets[t] = a.T[t];
+        for (size_t i = 0; i < a.kt.size(); ++i) {
+            q->bids.push_back(*s->free_bids.begin());
+            s->free_bids.erase(s->free_bids.begin());
+            need = std::max(need, a.keys[i] + 1);
+        }
+        result[k] = 0;
+        adm.push_back(std::move(a));
+    }
+    if (adm.empty()) return;
+    auto fail_admitted = [&](int e) {
+        for (size_t k = 0; k < nc; ++k)
+            if (result[k] == 0) result[k] = e;
+    };
+    // 3. column counts of every admitted bucket (all columns, dense columns)
+    std::vector<uint64_t> keys;
+    for (auto& a : adm) keys.insert(keys.end(), a.keys.begin(), a.keys.end());
+    const size_t nk = keys.size();
+    for (auto& a : adm)
+        for (size_t i = 0; i < a.kt.size(); ++i) {
+            const double Td = (double)a.T[a.kt[i]];
+            double qd = std::sqrt(Td) + 2;
+            for (int k = 0; k < 4; ++k) qd = std::sqrt(Td * std::log(std::max(qd, 3.0))) + 2;
+            keys.push_back(std::min<uint64_t>(qd >= 1.8e19 ? ~0ull : (uint64_t)qd, a.keys[i]));
+        }
+    int e = ensure_columns(c, need);
+    if (!e) e = ensure(c->keys, keys.size() * 8);
+    if (!e) e = ensure(c->counts, keys.size() * 8);
+    if (e) { fail_admitted(e); return; }
+    std::vector<uint64_t> cnt(keys.size());
+    if (cudaMemcpyAsync(c->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, c->st) != cudaSuccess) {
+        fail_admitted(WL_ERR_CUDA);
+        return;
+    }
+    launch_count_leq(as<uint32_t>(c->cols), c->ncols, as<uint64_t>(c->keys), (uint32_t)keys.size(),
+                     as<uint64_t>(c->counts), c->st);
+    s->ws.launches++;
+    if (cudaMemcpyAsync(cnt.data(), c->counts.p, keys.size() * 8, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+        cudaStreamSynchronize(c->st) != cudaSuccess) {
+        cudaGetLastError();
+        fail_admitted(WL_ERR_CUDA);
+        return;
+    }
+    // 4. buckets, rows and tail items on the host (tail items indexed globally
+    // in the admission's tail buffer)
+    std::vector<std::vector<RowInfo>> ris(adm.size());
+    std::vector<uint64_t> Ks(adm.size(), 1), item_off(adm.size(), 0), nitems(adm.size(), 0);
+    uint64_t items_total = 0;
+    size_t ki = 0;
+    for (size_t ai = 0; ai < adm.size(); ++ai) {
+        Adm& a = adm[ai];
+        SReq* q = a.q;
+        const bool full = q->qcap == 0;
+        std::vector<RowInfo>& ri = ris[ai];
+        ri.resize(q->nrows);
+        uint32_t row = q->r0;
+        uint64_t Wt = 0;
+        for (size_t i = 0; i < a.kt.size(); ++i, ++ki) {
+            const int t = a.kt[i];
+            const uint32_t bid = q->bids[i];
+            SBucket& b = s->sb[bid];
+            b.used = true;
+            b.ncols = cnt[ki];
+            b.cdense = std::min(cnt[nk + ki], cnt[ki]);
+            b.pos = 0;
+            b.nrows = (uint32_t)a.byc[t].size();
+            b.L = (uint32_t)q->L;
+            Bucket& d = s->pdesc[bid];
+            memset(&d, 0, sizeof(d));
+            d.T = a.T[t];
+            d.row_begin = row;
+            d.nrows = b.nrows;
+            d.L = b.L;
+            d.type = (uint32_t)t;
+            q->cells += (uint64_t)b.nrows * b.ncols;
+            for (uint64_t p : a.byc[t]) {
+                RowInfo& x = ri[row - q->r0];
+                uint32_t tt;
+                x.p = p;
+                x.Tp = class_target(p, &tt);
+                x.type = (uint32_t)t;
+                x.bucket = bid;
+                x.it_begin = 0;
+                x.it_count = 0;
+                if (full) Wt += x.Tp - d.T;
+                q->primes.push_back(p);
+                q->types.push_back((uint32_t)t);
+                ++row;
+            }
+        }
+        q->cells += Wt;
+        if (full && Wt) {
+            uint64_t K = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)Wt / ((double)c->sms * 2048.0 * 2.0)));
+            K = std::min<uint64_t>(K, 1u << 30);
+            uint64_t ni = 0;
+            for (uint32_t k = 0; k < q->nrows; ++k) {
+                const uint64_t len = ri[k].Tp - s->pdesc[ri[k].bucket].T;
+                ri[k].it_begin = (uint32_t)(items_total + ni);
+                ri[k].it_count = (uint32_t)((len + K - 1) / K);
+                ni += ri[k].it_count;
+            }
+            Ks[ai] = K;
+            item_off[ai] = items_total;
+            nitems[ai] = ni;
+            items_total += ni;
+        }
+    }
+    if (items_total >= (1ull << 32)) { fail_admitted(WL_ERR_UNSUPPORTED); return; }
+    if (items_total && (e = ensure(s->ipart, items_total * 16 + 16))) { fail_admitted(e); return; }
+    // 5. uploads (the stream is idle), then the launches, one synchronisation
+    bool ok = true;
+    for (size_t ai = 0; ai < adm.size() && ok; ++ai) {
+        SReq* q = adm[ai].q;
+        ok &= cudaMemcpyAsync(as<RowInfo>(s->info) + q->r0, ris[ai].data(), (size_t)q->nrows * sizeof(RowInfo),
+                              cudaMemcpyHostToDevice, c->st) == cudaSuccess;
+        for (uint32_t bid : q->bids) {
+            ok &= cudaMemcpyAsync(as<Bucket>(s->pbuckets) + bid, &s->pdesc[bid], sizeof(Bucket),
+                                  cudaMemcpyHostToDevice, c->st) == cudaSuccess;
+            ok &= cudaMemsetAsync(as<Deficit>(s->bdef) + bid, 0, sizeof(Deficit), c->st) == cudaSuccess;
+        }
+    }
+    for (size_t ai = 0; ai < adm.size() && ok; ++ai) {
+        SReq* q = adm[ai].q;
+        launch_setup_rows(as<RowInfo>(s->info) + q->r0, q->nrows, as<RowMod>(s->mods) + q->r0, c->st);
+        launch_acc_init(q->nrows, 0, as<uint4>(s->acc) + q->r0, nullptr, c->st);
+        s->ws.launches += 2;
+        if (nitems[ai]) {
+            launch_iterate(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), q->r0, q->nrows,
+                           (uint32_t)item_off[ai], (uint32_t)nitems[ai], Ks[ai], as<uint4>(s->ipart), c->st);
+            launch_tail_merge(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                              as<uint4>(s->ipart), Ks[ai], q->r0, q->nrows, as<uint4>(s->acc), as<Deficit>(s->bdef),
+                              c->st);
+            launch_clear_tail(as<RowInfo>(s->info), q->r0, q->nrows, c->st);
+            s->ws.launches += 3;
+        }
+    }
+    cudaEventRecord(s->e1, c->st);
+    if (!ok || cudaStreamSynchronize(c->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        cudaGetLastError();
+        fail_admitted(WL_ERR_CUDA);
+        return;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->e0, s->e1);
+    s->ws.ms_admit += ms;
+}
+
+// One scheduler step: every bucket with columns left advances by one chunk.
+static int serve_step(wl_server* s) {
+    wl_ctx* c = s->c;
+    struct Work { uint32_t bid; uint64_t c0, len; bool dense; };
+    std::vector<Work> work;
+    // the step's descriptor table covers every slot (a merge over a span of
+    // rows may meet stale bucket ids of freed rows): slots without work this
+    // step have nsplit = 0
+    const uint32_t top = s->bucket_cap;
+    size_t nact = 0;
+    for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && s->sb[bid].pos < s->sb[bid].ncols;
+    if (!nact) return 0;
+    // an equal share of the cell budget per bucket; a dense column costs
+    // about five cells (prefix fold + windowed buckets)
+    const double share = (double)s->step_cells / (double)nact;
+    double W = 0;
+    for (uint32_t bid = 0; bid < top; ++bid) {
+        SBucket& b = s->sb[bid];
+        if (!b.used || b.pos >= b.ncols) continue;
+        Work w;
+        w.bid = bid;
+        w.c0 = b.pos;
+        w.dense = b.pos < b.cdense;
+        const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
+        const uint64_t want = (uint64_t)std::max(share / per, w.dense ? 1024.0 : 8192.0);
+        const uint64_t end = w.dense ? b.cdense : b.ncols;
+        w.len = std::min<uint64_t>(end - b.pos, want);
+        // do not leave a sliver behind
+        if (end - b.pos - w.len < w.len / 4) w.len = end - b.pos;
+        W += per * (double)w.len;
+        work.push_back(w);
+    }
+    const double target_threads = (double)c->sms * 2048.0 * 4.0;
+    std::vector<Bucket> sbk(top);
+    memset(sbk.data(), 0, sbk.size() * sizeof(Bucket));
+    struct Grp { int L, rpt; bool dense; std::vector<SweepItem> items; };
+    std::vector<Grp> groups;
+    uint64_t part_total = 0;
+    uint32_t def_total = 0;
+    std::vector<uint32_t> bucket_splits(top, 0);
+    for (const Work& w : work) {
+        const SBucket& b = s->sb[w.bid];
+        Bucket& x = sbk[w.bid];
+        x = s->pdesc[w.bid];
+        x.cbase = (uint32_t)w.c0;
+        x.ncols = (uint32_t)w.len;
+        int rpt = 1;
+        uint32_t tps = 256;
+        if (w.dense) {
+            dense_shape(b.nrows, &rpt, &tps);
+        } else {
+            if (b.nrows >= 512) rpt = c->tune.sparse_rpt[b.L - 2];
+            if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
+        }
+        const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
+        uint64_t S = (uint64_t)std::ceil((double)rpt * per / (double)b.nrows * (double)w.len *
+                                         target_threads / W);
+        const uint64_t minlen = w.dense ? 256 : 2048;
+        S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, w.len / minlen)));
+        if (w.dense) S = std::max<uint64_t>(S, std::min<uint64_t>((w.len + 1023) / 1024, w.len / 256 ? w.len / 256 : 1));
+        x.nsplit = (uint32_t)S;
+        x.cdense = w.dense ? (uint32_t)w.len : 0;
+        x.ndense = w.dense ? (uint32_t)S : 0;
+        x.dstart = 0;
+        x.part_base = part_total;
+        x.def_base = def_total;
+        part_total += S * b.nrows;
+        def_total += (uint32_t)S;
+        bucket_splits[w.bid] = (uint32_t)S;
+        Grp* g = nullptr;
+        for (auto& gg : groups)
+            if (gg.L == (int)b.L && gg.rpt == rpt && gg.dense == w.dense) g = &gg;
+        if (!g) {
+            groups.push_back({ (int)b.L, rpt, w.dense, {} });
+            g = &groups.back();
+        }
+        if (tps == 256) {
+            const uint32_t tile = 256 * rpt;
+            for (uint32_t r = 0; r < b.nrows; r += tile)
+                for (uint32_t s2 = 0; s2 < S; ++s2) g->items.push_back({ w.bid, r, s2, 256u });
+        } else {
+            const uint32_t per_cta = 256 / tps;
+            for (uint32_t s2 = 0; s2 < S; s2 += per_cta) g->items.push_back({ w.bid, 0, s2, tps });
+        }
+    }
+    std::vector<SweepItem> all;
+    for (auto& g : groups) all.insert(all.end(), g.items.begin(), g.items.end());
+    RC(ensure(s->sbuckets, sbk.size() * sizeof(Bucket)));
+    RC(ensure(c->items, all.size() * sizeof(SweepItem) + 16));
+    RC(ensure(c->part, part_total * 16 + 16));
+    RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
+    cudaEventRecord(s->e0, c->st);
+    CK(cudaMemcpyAsync(s->sbuckets.p, sbk.data(), sbk.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->items.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, c->st));
+    size_t ioff = 0;
+    for (auto& g : groups) {
+        if (g.dense)
+            launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
+                               as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(c->part),
+                               as<Deficit>(c->defs), c->st,
+                               c->tune.dense_kernel[g.L - 2], (uint32_t)c->tune.dense_hstep[g.L - 2]);
+        else
+            launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
+                         as<SweepItem>(c->items) + ioff, as<RowMod>(s->mods), as<uint32_t>(c->cols),
+                         as<uint4>(c->part), as<Deficit>(c->defs), c->st);
+        s->ws.launches++;
+        ioff += g.items.size();
+    }
+    // fold the chunk into the resident running products: one launch per limb
+    // width over the span of the active requests' rows (rows of buckets
+    // without splits this step, or not in use, are left alone by the kernel)
+    for (int L = 2; L <= 4; ++L) {
+        uint32_t lo = UINT32_MAX, hi = 0, maxs = 0;
+        for (SReq* q : s->active) {
+            if (q->L != L) continue;
+            uint32_t m = 0;
+            for (uint32_t bid : q->bids) if (bid < top) m = std::max(m, bucket_splits[bid]);
+            if (!m) continue;
+            maxs = std::max(maxs, m);
+            lo = std::min(lo, q->r0);
+            hi = std::max(hi, q->r0 + q->nrows);
+        }
+        if (!maxs) continue;
+        if (maxs >= (uint32_t)c->tune.merge_cta_min)
+            launch_merge_cta(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                             as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
+                             as<Deficit>(s->bdef), c->st);
+        else
+            launch_merge(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                         as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
+                         as<Deficit>(s->bdef), c->st);
+        s->ws.launches++;
+    }
+    cudaEventRecord(s->e1, c->st);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->e0, s->e1);
+    s->ws.ms_steps += ms;
+    s->ws.steps++;
+    for (const Work& w : work) s->sb[w.bid].pos += w.len;
+    return 0;
+}
+
+static int serve_finish(wl_server* s, SReq* q) {
+    wl_ctx* c = s->c;
+    const bool full = q->qcap == 0;
+    launch_finish(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), nullptr, nullptr, 1,
+                  nullptr, q->r0, q->nrows, full ? 1 : 0, as<RowOut>(s->out), c->st, as<uint4>(s->acc),
+                  as<Deficit>(s->bdef), nullptr, nullptr);
+    s->ws.launches++;
+    std::vector<RowOut> ro(q->nrows);
+    CK(cudaMemcpyAsync(ro.data(), as<RowOut>(s->out) + q->r0, (size_t)q->nrows * sizeof(RowOut),
+                       cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    std::vector<uint32_t> ord(q->nrows);
+    for (uint32_t k = 0; k < q->nrows; ++k) ord[k] = k;
+    std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return q->primes[a] < q->primes[b]; });
+    uint64_t ck = 0;
+    int err = 0;
+    q->rows.resize(q->nrows);
+    for (uint32_t j = 0; j < q->nrows; ++j) {
+        const uint32_t k = ord[j];
+        wl_row& w = q->rows[j];
+        memset(&w, 0, sizeof(w));
+        w.p = q->primes[k];
+        w.s0 = ro[k].s0;
+        w.s1 = ro[k].s1;
+        w.rem = ro[k].rem;
+        w.quot = ro[k].quot;
+        w.type = q->types[k];
+        w.status = ro[k].status;
+        if (full) {
+            ck += w.p + w.rem + w.quot;
+            int32_t v;
+            if (result_of(w, &v)) q->lines.push_back(wl_result{ w.p, v });
+            if (w.status == 1 && !err) err = WL_ERR_WILSON_CHECK;
+            if (w.status == 2 && !err) err = WL_ERR_NO_REPR;
+        } else {
+            ck += w.p + w.s0 + w.s1;
+        }
+    }
+    q->checksum = ck;
+    return err;
+}
+
+static void serve_end(wl_server* s, SReq* q, int state, int rc) {
+    // called with s->mu held
+    q->state = state;
+    q->rc = rc;
+    q->t_done = s->now_ms();
+    if (state == WL_REQ_DONE) { s->ws.completed++; s->ws.rows_done += q->rows.size(); s->ws.cells += q->cells; }
+    else if (state == WL_REQ_CANCELLED) s->ws.cancelled++;
+    else s->ws.failed++;
+    q->tested = state == WL_REQ_DONE ? q->rows.size() : 0;
+    s->stats = s->ws;
+    q->tps.clear();
+    q->tps.shrink_to_fit();
+    s->cv_done.notify_all();
+}
+
+static void serve_loop(wl_server* s) {
+    cudaSetDevice(s->c->device);
+    while (true) {
+        // admit queued requests in FIFO order while they fit, all at once
+        std::vector<SReq*> cands;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (!s->stop && s->queue.empty() && s->active.empty()) s->cv_work.wait(lk);
+            if (s->stop) return;
+            for (auto it = s->queue.begin(); it != s->queue.end();) {
+                if ((*it)->cancel) {
+                    serve_end(s, *it, WL_REQ_CANCELLED, 0);
+                    it = s->queue.erase(it);
+                } else {
+                    cands.push_back(*it);
+                    ++it;
+                }
+            }
+        }
+        if (!cands.empty()) {
+            std::vector<int> res;
+            serve_admit_batch(s, cands, res);
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (size_t k = 0; k < cands.size(); ++k) {
+                SReq* q = cands[k];
+                if (res[k] == 1) continue;                  // waits for rows to free up
+                s->queue.erase(std::find(s->queue.begin(), s->queue.end(), q));
+                if (res[k]) {
+                    serve_release(s, q);
+                    serve_end(s, q, WL_REQ_FAILED, res[k]);
+                    continue;
+                }
+                q->state = WL_REQ_ACTIVE;
+                q->t_admit = s->now_ms();
+                s->active.push_back(q);
+                q->tested = q->nrows;
+                s->ws.admitted++;
+            }
+            s->ws.peak_rows = std::max(s->ws.peak_rows, s->rows_used);
+            s->ws.peak_active = std::max<uint32_t>(s->ws.peak_active, (uint32_t)s->active.size());
+            s->stats = s->ws;
+        }
+        if (s->active.empty()) continue;
+        const int e = serve_step(s);
+        std::vector<SReq*> keep;
+        for (SReq* q : s->active) {
+            bool done = true;
+            for (uint32_t bid : q->bids) done &= s->sb[bid].pos >= s->sb[bid].ncols;
+            bool cancel;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                cancel = q->cancel;
+            }
+            if (!e && !cancel && !done) { keep.push_back(q); continue; }
+            int rc = e;
+            if (!e && !cancel) rc = serve_finish(s, q);
+            std::lock_guard<std::mutex> lk(s->mu);
+            serve_release(s, q);
+            serve_end(s, q, cancel ? WL_REQ_CANCELLED : (rc ? WL_REQ_FAILED : WL_REQ_DONE), cancel ? 0 : rc);
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->active.swap(keep);
+        s->stats = s->ws;
+    }
+}
+
+extern "C" {
+
+int wl_server_open(const wl_server_opts* opts, wl_server** out) {
+    if (!out) return WL_ERR_ARG;
+    *out = nullptr;
+    wl_server_opts o;
+    memset(&o, 0, sizeof(o));
+    if (opts) o = *opts;
+    const uint64_t bytes = o.pool_bytes ? o.pool_bytes : (1ull << 30);
+    if (bytes / WL_SERVER_ROW_BYTES < 1024) return WL_ERR_ARG;
+    wl_server* s = new wl_server();
+    int rc = wl_open(o.device, &s->c);
+    if (rc) { delete s; return rc; }
+    if (o.tuning && (rc = wl_set_tuning(s->c, o.tuning))) {
+        wl_close(s->c);
+        delete s;
+        return rc;
+    }
+    s->pool_cap = (uint32_t)std::min<uint64_t>(bytes / WL_SERVER_ROW_BYTES, 1u << 30);
+    s->step_cells = o.step_cells ? o.step_cells : (1ull << 32);
+    s->bucket_cap = 3 * 1024;
+    s->sb.assign(s->bucket_cap, SBucket());
+    s->pdesc.resize(s->bucket_cap);
+    memset(s->pdesc.data(), 0, s->pdesc.size() * sizeof(Bucket));
+    for (uint32_t b = 0; b < s->bucket_cap; ++b) s->free_bids.insert(b);
+    s->free_rows[0] = s->pool_cap;
+    if (ensure(s->info, (size_t)s->pool_cap * sizeof(RowInfo)) || ensure(s->mods, (size_t)s->pool_cap * sizeof(RowMod)) ||
+        ensure(s->acc, (size_t)s->pool_cap * 16) || ensure(s->out, (size_t)s->pool_cap * sizeof(RowOut)) ||
+        ensure(s->pbuckets, s->bucket_cap * sizeof(Bucket)) || ensure(s->bdef, s->bucket_cap * sizeof(Deficit)) ||
+        cudaEventCreate(&s->e0) != cudaSuccess || cudaEventCreate(&s->e1) != cudaSuccess) {
+        cudaGetLastError();
+        DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->bdef };
+        for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+        wl_close(s->c);
+        delete s;
+        return WL_ERR_NOMEM;
+    }
+    cudaMemset(s->pbuckets.p, 0, s->bucket_cap * sizeof(Bucket));
+    cudaMemset(s->info.p, 0, (size_t)s->pool_cap * sizeof(RowInfo));   // bucket 0 for rows never admitted
+    s->worker = std::thread(serve_loop, s);
+    *out = s;
+    return 0;
+}
+
+int wl_server_submit(wl_server* s, uint64_t pmin, uint64_t pmax, uint64_t q_cap, uint64_t* id) {
+    if (!s) return WL_ERR_ARG;
+    RC(wl_check_range(pmin, pmax));
+    if (q_cap > (1ull << 32)) return WL_ERR_UNSUPPORTED;
+    SReq* q = new SReq();
+    q->pmin = pmin;
+    q->pmax = pmax;
+    q->qcap = q_cap;
+    std::lock_guard<std::mutex> lk(s->mu);
+    q->id = s->next_id++;
+    q->t_submit = s->now_ms();
+    s->reqs[q->id] = q;
+    s->queue.push_back(q);
+    if (id) *id = q->id;
+    s->cv_work.notify_all();
+    return 0;
+}
+
+static void fill_info(const SReq* q, wl_request_info* info) {
+    if (!info) return;
+    memset(info, 0, sizeof(*info));
+    info->id = q->id;
+    info->state = q->state;
+    info->rc = q->rc;
+    info->tested = q->tested;
+    // the scheduler writes these before the state changes (under the mutex)
+    if (q->state == WL_REQ_ACTIVE || q->state == WL_REQ_DONE) {
+        for (int t = 0; t < 3; ++t) info->targets[t] = q->targets[t];
+        info->cells = q->cells;
+    }
+    if (q->state == WL_REQ_DONE) {
+        info->checksum = q->checksum;
+        info->results = (uint32_t)q->lines.size();
+    }
+    info->ms_queued = q->t_admit > 0 ? q->t_admit - q->t_submit : 0;
+    info->ms_latency = q->t_done > 0 ? q->t_done - q->t_submit : 0;
+}
+
+static SReq* find_req(wl_server* s, uint64_t id) {
+    auto it = s->reqs.find(id);
+    return it == s->reqs.end() ? nullptr : it->second;
+}
+
+int wl_server_poll(wl_server* s, uint64_t id, wl_request_info* info) {
+    if (!s) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q) return WL_ERR_ARG;
+    fill_info(q, info);
+    return q->state >= WL_REQ_DONE ? 0 : 1;
+}
+
+int wl_server_wait(wl_server* s, uint64_t id, wl_request_info* info, double timeout_ms) {
+    if (!s) return WL_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q) return WL_ERR_ARG;
+    auto ended = [&] { return q->state >= WL_REQ_DONE; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, ended);
+    else s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ended);
+    fill_info(q, info);
+    return q->state >= WL_REQ_DONE ? 0 : 1;
+}
+
+int wl_server_results(wl_server* s, uint64_t id, wl_result* res, size_t cap, size_t* n) {
+    if (!s) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q || q->state != WL_REQ_DONE) return WL_ERR_ARG;
+    if (n) *n = q->lines.size();
+    if (res) memcpy(res, q->lines.data(), std::min(cap, q->lines.size()) * sizeof(wl_result));
+    return (res && cap < q->lines.size()) ? WL_ERR_CAPACITY : 0;
+}
+
+int wl_server_rows(wl_server* s, uint64_t id, wl_row* rows, size_t cap, size_t* n) {
+    if (!s) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q || q->state != WL_REQ_DONE) return WL_ERR_ARG;
+    if (n) *n = q->rows.size();
+    if (rows) memcpy(rows, q->rows.data(), std::min(cap, q->rows.size()) * sizeof(wl_row));
+    return (rows && cap < q->rows.size()) ? WL_ERR_CAPACITY : 0;
+}
+
+int wl_server_cancel(wl_server* s, uint64_t id) {
+    if (!s) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q) return WL_ERR_ARG;
+    q->cancel = true;
+    s->cv_work.notify_all();
+    return 0;
+}
+
+int wl_server_release(wl_server* s, uint64_t id) {
+    if (!s) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SReq* q = find_req(s, id);
+    if (!q || q->state < WL_REQ_DONE) return WL_ERR_ARG;
+    delete q;
+    s->reqs.erase(id);
+    return 0;
+}
+
+int wl_server_stats_get(wl_server* s, wl_server_stats* st) {
+    if (!s || !st) return WL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *st = s->stats;
+    return 0;
+}
+
+void wl_server_close(wl_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->c->device);
+    cudaStreamSynchronize(s->c->st);
+    DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->sbuckets, &s->bdef, &s->ipart };
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    if (s->e0) cudaEventDestroy(s->e0);
+    if (s->e1) cudaEventDestroy(s->e1);
+    for (auto& kv : s->reqs) delete kv.second;
+    wl_close(s->c);
+    delete s;
+}
+
+}  // extern "C"

@@ -125,7 +125,7 @@ SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", 
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
 PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5, "dfma": 6, "mad+dfma": 7,
-          "madwide+dfma": 8}
+          "madwide+dfma": 8, "cell2fp64": 9, "cell2mix": 10}
 
 _lib = None
 

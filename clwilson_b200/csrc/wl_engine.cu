@@ -552,7 +552,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     // the partial-product budget
     auto plan_splits = [&](size_t i, double scale, uint64_t* Sd_out, uint64_t* Ss_out) {
         const uint32_t nrows_b = (uint32_t)hb[i].primes.size();
-        const int rpt = nrows_b >= 512 ? c->tune.sparse_rpt[hb[i].L - 2] : 1;
+        const int rpt = sparse_rpt_for(c->tune.sparse_rpt[hb[i].L - 2], nrows_b);
         const uint64_t nd = ndn[i], ns = ncol[i] - nd;
         uint64_t Sd = 0, Ss = 0;
         if (nd > 0) {
@@ -604,7 +604,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         b.type = h.type;
         b.range = h.range;
         int rpt, tps;
-        if (b.nrows >= 512) { rpt = c->tune.sparse_rpt[b.L - 2]; tps = 256; }
+        if (b.nrows >= 512) { rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows); tps = 256; }
         else if (b.nrows >= 256) { rpt = 1; tps = 256; }
         else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
         const uint64_t nd = ndn[i];
@@ -1149,7 +1149,8 @@ int wl_get_tuning(wl_ctx* c, wl_tuning* out) {
 int wl_set_tuning(wl_ctx* c, const wl_tuning* t) {
     if (!c || !t) return WL_ERR_ARG;
     for (int i = 0; i < 3; ++i) {
-        if (t->sparse_variant[i] < 0 || t->sparse_variant[i] > 2 || t->sparse_rpt[i] < 1 || t->sparse_rpt[i] > 2 ||
+        if (t->sparse_variant[i] < 0 || t->sparse_variant[i] > 3 ||
+            (t->sparse_rpt[i] != 1 && t->sparse_rpt[i] != 2 && t->sparse_rpt[i] != 4) ||
             t->dense_kernel[i] < 0 || t->dense_kernel[i] > 5 || t->dense_hstep[i] < 1 || t->dense_hstep[i] > 4096)
             return WL_ERR_ARG;
     }
@@ -1206,7 +1207,8 @@ static int tune_on(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, uint3
         else c->tune = keep;
         return 0;
     };
-    const int sparse_c[3][2] = { { 1, 1 }, { 0, 2 }, { 2, 2 } };   // (variant, rows per thread) besides (1, 2)
+    // (variant, rows per thread) besides (1, 2)
+    const int sparse_c[5][2] = { { 1, 1 }, { 0, 2 }, { 2, 2 }, { 1, 4 }, { 3, 4 } };
     for (auto& sc : sparse_c) {
         wl_tuning t = c->tune;
         apply([&](int i) { t.sparse_variant[i] = sc[0]; t.sparse_rpt[i] = sc[1]; });

@@ -32,6 +32,14 @@ inline int ensure(DevBuf& b, size_t bytes) {
 
 template <class T> inline T* as(DevBuf& b) { return reinterpret_cast<T*>(b.p); }
 
+// Rows per thread of the prefix-fold sweep for a bucket of nrows rows, given
+// the tuned choice (1, 2 or 4): one row below 512 rows, at most two below 1,024.
+inline int sparse_rpt_for(int tuned, uint32_t nrows) {
+    if (nrows < 512) return 1;
+    if (tuned == 4 && nrows < 1024) return 2;
+    return tuned;
+}
+
 // Limb width of residues mod p^2 for primes up to pmax_incl.
 inline int limb_width(uint64_t pmax_incl) {
     if (pmax_incl < (1ull << 31)) return 2;

@@ -412,7 +412,7 @@ static int serve_step(wl_server* s) {
         if (w.dense) {
             dense_shape(b.nrows, &rpt, &tps);
         } else {
-            if (b.nrows >= 512) rpt = c->tune.sparse_rpt[b.L - 2];
+            rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows);
             if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
         }
         const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);

@@ -202,8 +202,10 @@ int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p
 #define WL_DENSE_SMEM_W3   4   /* digit-sorted, buckets in shared memory, 3-bit, 4 CTAs/SM */
 #define WL_DENSE_SMEM_W4   5   /* digit-sorted, buckets in shared memory, 4-bit, 2 CTAs/SM */
 typedef struct {
-    int32_t sparse_variant[3];   /* cell formulation of the prefix-fold sweep: 0 carry chain, 1 wide products, 2 high half first */
-    int32_t sparse_rpt[3];       /* rows per thread of the prefix-fold sweep for buckets of >= 512 rows (1 or 2) */
+    int32_t sparse_variant[3];   /* cell formulation of the prefix-fold sweep: 0 carry chain, 1 wide products,
+                                    2 high half first, 3 wide products with each thread's last row on the carry chain */
+    int32_t sparse_rpt[3];       /* rows per thread of the prefix-fold sweep for buckets of >= 512 rows (1, 2;
+                                    4 from 1,024 rows) */
     int32_t dense_kernel[3];     /* WL_DENSE_* */
     int32_t dense_hstep[3];      /* columns per change of the exponent's high part in the dense sweep */
     int32_t merge_cta_min;       /* split count from which partials merge with one CTA per row (tree fan-in 256) */

@@ -46,8 +46,8 @@ def test_dense_variants(eng, golden, kernel, hstep):
     _capped_ok(eng, golden, (1 << 62) - 1 - 10**7, (1 << 62) - 1, 1 << 16)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
-@pytest.mark.parametrize("rpt", [1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("rpt", [1, 2, 4])
 @pytest.mark.parametrize("merge", [1, 10**6])
 def test_sparse_variants_full_search(eng, golden, big_rows, variant, rpt, merge):
     eng.tuning = {"sparse_variant": [variant] * 3, "sparse_rpt": [rpt] * 3, "merge_cta_min": merge,
@@ -68,6 +68,8 @@ def test_set_tuning_rejects_bad_values(eng):
         eng.tuning = {"dense_kernel": [7, 0, 0]}
     with pytest.raises(wl.WilsonError):
         eng.tuning = {"sparse_rpt": [3, 1, 1]}
+    with pytest.raises(wl.WilsonError):
+        eng.tuning = {"sparse_variant": [4, 1, 1]}
 
 
 def test_autotune_and_serving_with_tuning(eng):

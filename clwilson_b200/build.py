@@ -63,8 +63,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         os.replace(tmp, LIB)
     cli_src = os.path.join(CSRC, "wl_cli.cpp")
-    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB, os.path.join(INCLUDE, "wilson.h")])):
-        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, cli_src, "-o", CLI + ".tmp",
+    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB, os.path.join(INCLUDE, "wilson.h"),
+                                                            os.path.join(CSRC, "wl_ckpt.h")])):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, "-I", CSRC, cli_src, "-o", CLI + ".tmp",
                "-L", PKG, "-lwilson", "-Wl,-rpath,$ORIGIN"]
         subprocess.check_call(cmd)
         os.replace(CLI + ".tmp", CLI)

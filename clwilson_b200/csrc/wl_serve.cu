@@ -14,6 +14,7 @@
 #include "wilson.h"
 #include "wl_internal.h"
 #include "wl_host.h"
+#include "wl_pool.h"
 
 using namespace wl;
 
@@ -74,9 +75,8 @@ struct wl_server {
     DevBuf info, mods, acc, out, pbuckets, sbuckets, bdef, ipart;
     std::vector<SBucket> sb;
     std::vector<Bucket> pdesc;                 // persistent descriptors (device copy: pbuckets)
-    std::map<uint32_t, uint32_t> free_rows;    // first row -> length
+    RowPool pool;                              // rows of the device row pool
     std::set<uint32_t> free_bids;
-    uint32_t rows_used = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<SReq*> queue;
@@ -94,36 +94,6 @@ struct wl_server {
     }
 };
 
-static bool pool_alloc(wl_server* s, uint32_t n, uint32_t* r0) {
-    for (auto it = s->free_rows.begin(); it != s->free_rows.end(); ++it) {
-        if (it->second < n) continue;
-        *r0 = it->first;
-        const uint32_t rest = it->second - n, start = it->first + n;
-        s->free_rows.erase(it);
-        if (rest) s->free_rows[start] = rest;
-        s->rows_used += n;
-        return true;
-    }
-    return false;
-}
-
-static void pool_free(wl_server* s, uint32_t r0, uint32_t n) {
-    s->rows_used -= n;
-    auto it = s->free_rows.emplace(r0, n).first;
-    auto nx = std::next(it);
-    if (nx != s->free_rows.end() && it->first + it->second == nx->first) {
-        it->second += nx->second;
-        s->free_rows.erase(nx);
-    }
-    if (it != s->free_rows.begin()) {
-        auto pv = std::prev(it);
-        if (pv->first + pv->second == it->first) {
-            pv->second += it->second;
-            s->free_rows.erase(it);
-        }
-    }
-}
-
 static void serve_release(wl_server* s, SReq* q) {
     for (uint32_t bid : q->bids) {
         s->sb[bid] = SBucket();
@@ -131,7 +101,7 @@ static void serve_release(wl_server* s, SReq* q) {
         s->free_bids.insert(bid);
     }
     q->bids.clear();
-    if (q->nrows) pool_free(s, q->r0, q->nrows);
+    if (q->nrows) s->pool.release(q->r0, q->nrows);
     q->nrows = 0;
 }
 
@@ -210,7 +180,7 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
         }
         if (unsupported) { result[k] = WL_ERR_UNSUPPORTED; continue; }
         uint32_t r0 = 0;
-        if (s->free_bids.size() < a.kt.size() || !pool_alloc(s, n, &r0)) break;
+        if (s->free_bids.size() < a.kt.size() || !s->pool.alloc(n, &r0)) break;
         q->r0 = r0;
         q->nrows = n;
         q->L = limb_width(q->pmax - 1);
@@ -601,7 +571,7 @@ static void serve_loop(wl_server* s) {
                 q->tested = q->nrows;
                 s->ws.admitted++;
             }
-            s->ws.peak_rows = std::max(s->ws.peak_rows, s->rows_used);
+            s->ws.peak_rows = std::max(s->ws.peak_rows, s->pool.used);
             s->ws.peak_active = std::max<uint32_t>(s->ws.peak_active, (uint32_t)s->active.size());
             s->stats = s->ws;
         }
@@ -654,7 +624,7 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
     s->pdesc.resize(s->bucket_cap);
     memset(s->pdesc.data(), 0, s->pdesc.size() * sizeof(Bucket));
     for (uint32_t b = 0; b < s->bucket_cap; ++b) s->free_bids.insert(b);
-    s->free_rows[0] = s->pool_cap;
+    s->pool.reset(s->pool_cap);
     if (ensure(s->info, (size_t)s->pool_cap * sizeof(RowInfo)) || ensure(s->mods, (size_t)s->pool_cap * sizeof(RowMod)) ||
         ensure(s->acc, (size_t)s->pool_cap * 16) || ensure(s->out, (size_t)s->pool_cap * sizeof(RowOut)) ||
         ensure(s->pbuckets, s->bucket_cap * sizeof(Bucket)) || ensure(s->bdef, s->bucket_cap * sizeof(Deficit)) ||

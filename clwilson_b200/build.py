@@ -17,7 +17,7 @@ LIB = os.path.join(PKG, "libwilson.so")
 CLI = os.path.join(PKG, "clwilson")
 
 CU_SOURCES = ["wl_kernels.cu", "wl_engine.cu", "wl_serve.cu", "wl_probe.cu", "wl_noalloc.cu"]
-HEADERS = ["wl_arith.cuh", "wl_internal.h", "wl_host.h", "wl_pool.h", "wl_ckpt.h"]
+HEADERS = ["wl_arith.cuh", "wl_internal.h", "wl_host.h", "wl_pool.h", "wl_ckpt.h", "wl_plan.h"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -29,6 +29,7 @@
 #include "wilson.h"
 #include "wl_internal.h"
 #include "wl_host.h"
+#include "wl_plan.h"
 
 using namespace wl;
 
@@ -37,37 +38,6 @@ namespace {
 uint64_t pi_upper_bound(uint64_t x) {   // Rosser-Schoenfeld: pi(x) < 1.25506 x / ln x for x > 1
     if (x < 64) return 64;
     return (uint64_t)(1.2551 * (double)x / std::log((double)x)) + 64;
-}
-
-// Cells per row that a dense column at prime q costs for class target T: one
-// for the prefix product plus 7/8 of one per 3-bit window of the exponent's
-// low part, s ~ log2(8 T ln(q) / q^2) bits when the high part changes every 8
-// columns (k_sweep_dense), at most the exponent's length.
-double dense_cells_at(double T, double q) {
-    const double e = T / (q - 1.0);
-    double sb = std::log2(std::max(1.0, 8.0 * T * std::log(q) / (q * q)));
-    sb = std::min(sb, std::log2(std::max(e, 1.0)) + 1.0);
-    return 1.0 + 0.875 * std::ceil(sb / 3.0);
-}
-
-// Cumulative dense cost over q in [2, qd] on a log grid: cum[k] for q = grid[k].
-void dense_cost_grid(double T, double qd, std::vector<double>& grid, std::vector<double>& cum, double* cols_est) {
-    const int N = 2048;
-    grid.assign(N + 1, 0.0);
-    cum.assign(N + 1, 0.0);
-    const double u0 = std::log(2.0), u1 = std::log(std::max(qd, 3.0));
-    const double du = (u1 - u0) / N;
-    double c = 0, n = 0;
-    grid[0] = 2.0;
-    for (int k = 1; k <= N; ++k) {
-        const double u = u0 + (k - 0.5) * du, q = std::exp(u);
-        const double dn = q * du / u;            // primes in the step ~ dq / ln q
-        n += dn;
-        c += dn * dense_cells_at(T, q);
-        grid[k] = std::exp(u0 + k * du);
-        cum[k] = c;
-    }
-    *cols_est = n;
 }
 
 }  // namespace
@@ -621,21 +591,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         // q_k), interpolated inside a grid step: there are more splits than grid
         // points when the dense region is long, and a boundary snapped to the
         // grid would leave empty splits next to ones many times too long
-        for (uint64_t k = 1; k < Sd && !cb_lo[i]; ++k) {
-            const std::vector<double>& cum = dcum[i];
-            const std::vector<double>& grid = dgrid[i];
-            const double target = cum.back() * (double)k / (double)Sd;
-            size_t j = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
-            if (j >= cum.size()) j = cum.size() - 1;
-            double q = grid[j];
-            if (j > 0 && cum[j] > cum[j - 1]) {
-                // the cost per unit of ln q grows about like q inside a step:
-                // linear in q between the grid points
-                const double f = (target - cum[j - 1]) / (cum[j] - cum[j - 1]);
-                q = grid[j - 1] + f * (grid[j] - grid[j - 1]);
-            }
-            dkeys.push_back((uint64_t)q);
-        }
+        for (uint64_t k = 1; k < Sd && !cb_lo[i]; ++k)
+            dkeys.push_back((uint64_t)dense_boundary(dgrid[i], dcum[i], k, Sd));
         b.nsplit = (uint32_t)(Sd + Ss);
         const uint64_t S = b.nsplit;
         b.part_base = part_total;

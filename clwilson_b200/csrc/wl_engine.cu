@@ -517,51 +517,26 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         groups.push_back({ L, rpt, dense, {} });
         return groups.back().items;
     };
-    // splits per bucket: dense (Sd) and sparse (Ss); `scale` < 1 lengthens all
-    // splits when the split partials (16 bytes per split and row) would not fit
-    // the partial-product budget
-    auto plan_splits = [&](size_t i, double scale, uint64_t* Sd_out, uint64_t* Ss_out) {
-        const uint32_t nrows_b = (uint32_t)hb[i].primes.size();
-        const int rpt = sparse_rpt_for(c->tune.sparse_rpt[hb[i].L - 2], nrows_b);
-        const uint64_t nd = ndn[i], ns = ncol[i] - nd;
-        uint64_t Sd = 0, Ss = 0;
-        if (nd > 0) {
-            // dense splits of equal estimated cost, 256 to 1024 columns long so
-            // that the per-split bucket combination stays small
-            Sd = (uint64_t)std::ceil(dcost[i] * target_threads / W);
-            Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
-            Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
-            Sd = std::max<uint64_t>(1, (uint64_t)((double)Sd * scale));
-        }
-        if (ns > 0) {
-            Ss = (uint64_t)std::ceil((double)rpt * (double)ns * target_threads / W);
-            // at most 2^17 columns per split: a bucket whose share of the threads
-            // is small (few rows next to much dense work) would otherwise run as a
-            // few very long CTAs that finish long after everything else
-            Ss = std::max<uint64_t>(Ss, (ns + (1u << 17) - 1) >> 17);
-            Ss = std::max<uint64_t>(1, std::min<uint64_t>(Ss, std::max<uint64_t>(1, ns / 2048)));
-            Ss = std::max<uint64_t>(1, (uint64_t)((double)Ss * scale));
-        }
-        if (Sd + Ss == 0) Ss = 1;
-        *Sd_out = Sd;
-        *Ss_out = Ss;
-    };
+    // splits per bucket (wl_plan.h), lengthened when the split partials would
+    // not fit a third of the free device memory (24 GiB at most)
+    std::vector<SplitBucket> sbs(nb);
+    for (size_t i = 0; i < nb; ++i) {
+        sbs[i].nrows = (uint32_t)hb[i].primes.size();
+        sbs[i].rpt = sparse_rpt_for(c->tune.sparse_rpt[hb[i].L - 2], sbs[i].nrows);
+        sbs[i].ndense = ndn[i];
+        sbs[i].nsparse = ncol[i] - ndn[i];
+        sbs[i].dcost = dcost[i];
+    }
     double scale = 1.0;
     {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); free_b = 8ull << 30; }
         const double budget = std::min<double>((double)(free_b + c->part.cap) / 3.0, 24.0 * (1ull << 30)) / 16.0;
-        for (int it = 0; it < 8; ++it) {
-            double tot = 0;
-            for (size_t i = 0; i < nb; ++i) {
-                uint64_t a, b2;
-                plan_splits(i, scale, &a, &b2);
-                tot += (double)(a + b2) * (double)hb[i].primes.size();
-            }
-            if (tot <= budget) break;
-            scale *= 0.9 * budget / tot;
-        }
+        scale = split_scale(sbs, W, target_threads, budget);
     }
+    auto plan_splits = [&](size_t i, double sc, uint64_t* Sd_out, uint64_t* Ss_out) {
+        plan_bucket_splits(sbs[i], W, target_threads, sc, Sd_out, Ss_out);
+    };
     for (uint32_t oi = 0; oi < border.size(); ++oi) {
         const uint32_t i = border[oi];
         const HostBucket& h = hb[i];

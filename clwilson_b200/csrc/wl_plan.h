@@ -1,4 +1,5 @@
-// wl_plan.h -- the cost model behind the dense sweep's split boundaries.
+// wl_plan.h -- split planning of the column sweeps: how many splits each
+// bucket gets, and the cost model behind the dense sweep's split boundaries.
 // Host code only (no CUDA).
 #pragma once
 #include <algorithm>
@@ -53,4 +54,59 @@ inline double dense_boundary(const std::vector<double>& grid, const std::vector<
         q = grid[j - 1] + f * (grid[j] - grid[j - 1]);
     }
     return q;
+}
+
+// One bucket as the split planner sees it.
+struct SplitBucket {
+    uint32_t nrows = 0;     // test primes of the bucket
+    int rpt = 1;            // rows per thread of its prefix-fold sweep
+    uint64_t ndense = 0;    // columns of the dense regime
+    uint64_t nsparse = 0;   // columns of the prefix-fold regime
+    double dcost = 0;       // modelled cells per row of its dense columns
+};
+
+// Dense (Sd) and prefix-fold (Ss) splits of one bucket for work W (row x
+// column cells of all buckets) spread over `threads` thread-splits; `scale`
+// < 1 lengthens every split (memory budget).
+//   dense: equal estimated cost, 256 to 1,024 columns each, so that the
+//          per-split combination of window buckets stays small;
+//   prefix-fold: at least 2,048 columns, at most 2^17 -- a bucket whose share
+//          of the threads is small (few rows next to much dense work) would
+//          otherwise run as a few very long CTAs that finish after the rest.
+inline void plan_bucket_splits(const SplitBucket& b, double W, double threads, double scale, uint64_t* Sd_out,
+                               uint64_t* Ss_out) {
+    const uint64_t nd = b.ndense, ns = b.nsparse;
+    uint64_t Sd = 0, Ss = 0;
+    if (nd > 0) {
+        Sd = (uint64_t)std::ceil(b.dcost * threads / W);
+        Sd = std::max<uint64_t>(Sd, (nd + 1023) / 1024);
+        Sd = std::max<uint64_t>(1, std::min<uint64_t>(Sd, std::max<uint64_t>(1, nd / 256)));
+        Sd = std::max<uint64_t>(1, (uint64_t)((double)Sd * scale));
+    }
+    if (ns > 0) {
+        Ss = (uint64_t)std::ceil((double)b.rpt * (double)ns * threads / W);
+        Ss = std::max<uint64_t>(Ss, (ns + (1u << 17) - 1) >> 17);
+        Ss = std::max<uint64_t>(1, std::min<uint64_t>(Ss, std::max<uint64_t>(1, ns / 2048)));
+        Ss = std::max<uint64_t>(1, (uint64_t)((double)Ss * scale));
+    }
+    if (Sd + Ss == 0) Ss = 1;
+    *Sd_out = Sd;
+    *Ss_out = Ss;
+}
+
+// The split-length scale (<= 1) that keeps the split partials -- one per split
+// and row -- within `budget` partials.
+inline double split_scale(const std::vector<SplitBucket>& bs, double W, double threads, double budget) {
+    double scale = 1.0;
+    for (int it = 0; it < 8; ++it) {
+        double tot = 0;
+        for (const SplitBucket& b : bs) {
+            uint64_t a, c;
+            plan_bucket_splits(b, W, threads, scale, &a, &c);
+            tot += (double)(a + c) * (double)b.nrows;
+        }
+        if (tot <= budget) break;
+        scale *= 0.9 * budget / tot;
+    }
+    return scale;
 }

@@ -1,10 +1,15 @@
-"""Dense split boundaries on the CPU (clwilson_b200/csrc/wl_plan.h).
+"""Split planning on the CPU (clwilson_b200/csrc/wl_plan.h).
 
-The boundaries must be strictly increasing and fall at equal shares of the
-cost model's cumulative cost, also when a bucket has many more dense splits
-than the cost grid has points (about 14,000 splits against 2,048 points for
-the batched workload's 4-limb buckets): boundaries snapped to grid points
-there left empty splits next to ones many times too long."""
+* Dense split boundaries are strictly increasing and fall at equal shares of
+  the cost model's cumulative cost, also when a bucket has many more dense
+  splits than the cost grid has points (about 14,000 splits against 2,048
+  points for the batched workload's 4-limb buckets): boundaries snapped to grid
+  points there left empty splits next to ones many times too long.
+* Split counts keep dense splits at 256 to 1,024 columns and prefix-fold splits
+  at 2,048 to 2^17 columns.
+* The memory budget lengthens splits so that the partials of the full
+  top-of-range workload (2.3e5 rows, 2e8 dense columns) fit; without it the
+  1,024-column rule asks for about 740 GB."""
 import os
 import subprocess
 
@@ -27,7 +32,8 @@ def driver(tmp_path_factory):
     (5.0e8, 7.4e4, 64),               # plain-small, type 2
 ])
 def test_boundaries_increase_at_equal_cost(driver, T, qd, Sd):
-    out = subprocess.run([driver, repr(T), repr(qd), str(Sd)], capture_output=True, text=True, check=True).stdout
+    out = subprocess.run([driver, "bounds", repr(T), repr(qd), str(Sd)], capture_output=True, text=True,
+                         check=True).stdout
     lines = out.strip().splitlines()
     grid_n, total = int(lines[0].split()[1]), float(lines[0].split()[3])
     pts = [tuple(map(float, ln.split())) for ln in lines[1:]]
@@ -40,3 +46,38 @@ def test_boundaries_increase_at_equal_cost(driver, T, qd, Sd):
     if Sd > grid_n:
         # far more distinct boundaries than grid points
         assert len(set(qs)) == Sd - 1
+
+
+THREADS = 148 * 2048 * 4.0
+
+
+def _splits(driver, *args):
+    out = subprocess.run([driver, "splits", *map(str, args)], capture_output=True, text=True, check=True).stdout
+    return tuple(map(int, out.split()))
+
+
+@pytest.mark.parametrize("nrows,nd,ns,share", [(48000, 0, 26_000_000, 0.5), (22, 14_000_000, 0, 0.001),
+                                               (22, 400_000, 14_000_000, 0.001), (100_000, 0, 5_000, 1.0)])
+def test_split_lengths(driver, nrows, nd, ns, share):
+    dcost = 5.0 * nd
+    W = (nrows * (ns + dcost)) / share            # this bucket's share of all work
+    Sd, Ss = _splits(driver, nrows, 2 if nrows >= 512 else 1, nd, ns, dcost, W, THREADS, 1.0)
+    if nd:
+        assert 256 <= nd / Sd <= 1024 or Sd == 1
+    if ns:
+        assert ns / Ss <= (1 << 17) + 1 and (ns / Ss >= 2048 or Ss == 1)
+    assert Sd + Ss >= 1
+
+
+def test_memory_budget_top_of_range(driver):
+    # 3 buckets of the full top-of-range workload (all columns dense below 2^32)
+    buckets = [(78000, 203_000_000, 0, 4.5 * 203_000_000)] * 3
+    W = sum(n * (ns + dc) for n, nd, ns, dc in buckets)
+    budget = 24 * 2**30 / 16
+    args = [W, THREADS, budget] + [x for b in buckets for x in b]
+    sc, tot = map(float, subprocess.run([driver, "scale", *map(str, args)], capture_output=True, text=True,
+                                        check=True).stdout.split())
+    assert sc < 0.05 and tot <= budget   # about 1.6e9 partials allowed against 4.6e10 asked
+    # unscaled, the 1,024-column rule alone would ask for ~740 GB of partials
+    Sd, _ = _splits(driver, 78000, 2, 203_000_000, 0, 4.5 * 203_000_000, W, THREADS, 1.0)
+    assert Sd * 78000 * 3 * 16 > 700e9

@@ -120,7 +120,8 @@ assert ROW_DTYPE.itemsize == ctypes.sizeof(_Row)
 
 # exported symbols of include/wilson.h
 SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", "wl_search", "wl_rows",
-           "wl_batch", "wl_rows_from", "wl_search_from", "wl_drop_columns", "wl_parse_uint64", "wl_probe",
+           "wl_batch", "wl_rows_from", "wl_search_from", "wl_rows_product", "wl_drop_columns", "wl_parse_uint64",
+           "wl_probe",
            "wl_column_product_noalloc", "wl_get_tuning", "wl_set_tuning", "wl_autotune",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
@@ -160,6 +161,8 @@ def load_library(path: str = LIB_PATH):
     L.wl_rows_from.restype = ctypes.c_int
     L.wl_search_from.argtypes = [vp, u64, u64, u64, vp, ctypes.POINTER(_Result), sz, ctypes.POINTER(_Stats)]
     L.wl_search_from.restype = ctypes.c_int
+    L.wl_rows_product.argtypes = [vp, sz, vp, sz, vp, vp]
+    L.wl_rows_product.restype = ctypes.c_int
     L.wl_parse_uint64.argtypes = [ctypes.POINTER(u64), ctypes.c_char_p, u64, u64]
     L.wl_parse_uint64.restype = ctypes.c_int
     L.wl_drop_columns.argtypes = [vp]
@@ -388,6 +391,35 @@ class Engine:
             raise WilsonError(rc, "wl_search_from")
         out = [(res[i].p, res[i].value) for i in range(min(st.results, cap))]
         return SearchResult(out, st.checksum, Stats.from_c(st))
+
+    def rows_product(self, parts) -> np.ndarray:
+        """Row-wise product of partial column products (wl_rows_product).
+
+        `parts`: row arrays of one range (wl_rows_from pieces over disjoint
+        column intervals, same primes in the same order).  Returns rows with
+        p and the digits (s0, s1) of the product mod p^2, the init of the
+        finishing search_from."""
+        parts = list(parts)
+        if not parts:
+            raise ValueError("rows_product needs at least one part")
+        p = np.ascontiguousarray(parts[0]["p"], dtype=np.uint64)
+        for x in parts[1:]:
+            if not np.array_equal(x["p"], p):
+                raise ValueError("rows_product: the parts hold different primes")
+        n = p.size
+        digits = np.ascontiguousarray(
+            np.stack([np.stack([np.asarray(x["s0"], dtype=np.uint64), np.asarray(x["s1"], dtype=np.uint64)], axis=1)
+                      for x in parts]))
+        out = np.zeros((max(n, 1), 2), dtype=np.uint64)
+        rc = self._L.wl_rows_product(self._ctx, n, p.ctypes.data, len(parts), digits.ctypes.data, out.ctypes.data)
+        if rc:
+            raise WilsonError(rc, "wl_rows_product")
+        rows = np.zeros(n, dtype=ROW_DTYPE)
+        rows["p"] = p
+        rows["s0"] = out[:n, 0]
+        rows["s1"] = out[:n, 1]
+        rows["type"] = parts[0]["type"]
+        return rows
 
     def batch(self, ranges: Sequence[Tuple[int, int]], q_cap: int = 0, cap: int = 1 << 20):
         n = len(ranges)

@@ -15,8 +15,9 @@
 //      (k_iterate), and the class lift + quotient (k_finish);
 //   5. results.txt lines (ascending p) and the checksum on the host
 //      (cl_wilson.cpp:872-900).
-// Also here: searches in pieces (q_lo / init of run_ranges), kernel tuning,
-// and the C ABI; serving sessions are in wl_serve.cu.
+// Also here: searches in pieces (q_lo / init of run_ranges) and the
+// row-wise product of pieces (wl_rows_product), kernel tuning, and the C ABI;
+// serving sessions are in wl_serve.cu.
 #include <algorithm>
 #include <cerrno>
 #include <cstdlib>
@@ -985,7 +986,7 @@ void wl_close(wl_ctx* c) {
                        &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
                        &c->bbitmap, &c->bsegcount, &c->boffsets, &c->boffs, &c->wcols, &c->wbuckets, &c->witems,
                        &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts, &c->uacc, &c->udef,
-                       &c->defs, &c->rowout };
+                       &c->defs, &c->rowout, &c->prod };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->fork) cudaEventDestroy(c->fork);
@@ -1061,6 +1062,30 @@ int wl_search_from(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_lo, const
     RunOut ro;
     RC(run_ranges(c, &r, 1, 0, ro, stats, q_lo, init));
     return summarize(ro, 1, true, nullptr, results, cap, nullptr, stats);
+}
+
+int wl_rows_product(wl_ctx* c, size_t n, const uint64_t* p, size_t nparts, const uint64_t* parts, uint64_t* out) {
+    if (!c || nparts == 0 || nparts > (1u << 16) || n > (1ull << 32)) return WL_ERR_ARG;
+    if (n == 0) return 0;
+    if (!p || !parts || !out) return WL_ERR_ARG;
+    for (size_t i = 0; i < n; ++i) {
+        if (p[i] < 5 || p[i] > WL_MAXP || !(p[i] & 1)) return WL_ERR_ARG;
+        for (size_t k = 0; k < nparts; ++k)
+            if (parts[k * 2 * n + 2 * i] >= p[i] || parts[k * 2 * n + 2 * i + 1] >= p[i]) return WL_ERR_ARG;
+    }
+    cudaSetDevice(c->device);
+    const size_t pb = n * 8, xb = nparts * n * 16, ob = n * 16;
+    RC(ensure(c->prod, pb + xb + ob));
+    uint64_t* dp = as<uint64_t>(c->prod);
+    uint64_t* dx = dp + n;
+    uint64_t* dout = dx + 2 * nparts * n;
+    CK(cudaMemcpyAsync(dp, p, pb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dx, parts, xb, cudaMemcpyHostToDevice, c->st));
+    launch_rows_product(dp, n, dx, (uint32_t)nparts, dout, c->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, ob, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
 }
 
 int wl_batch(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, wl_range_result* out,

@@ -163,5 +163,8 @@ void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowM
                    uint32_t row_begin, uint32_t nrows, int full, RowOut* out, cudaStream_t st,
                    const uint4* acc1 = nullptr, const Deficit* def1 = nullptr,
                    const uint4* acc2 = nullptr, const Deficit* def2 = nullptr);
+// out = row-wise product of nparts partial products (digits s0, s1 per row)
+void launch_rows_product(const uint64_t* ps, uint64_t n_rows, const uint64_t* parts, uint32_t nparts, uint64_t* out,
+                         cudaStream_t st);
 
 }  // namespace wl

@@ -1088,6 +1088,59 @@ k_finish(const Bucket* __restrict__ buckets, const RowInfo* __restrict__ info, c
 }
 
 // ===========================================================================
+// Row-wise product of partial column products.  When the column interval of
+// one range is split between GPUs, each returns per-row partial products as
+// values s0 + p*s1 < p^2; their product is the running product over the union
+// of the pieces (the role of reduce.cl:11-44, which folds work-group partials
+// into a residue, one level up).  parts[k * 2n + 2i + {0, 1}] = digits of row
+// i's k-th partial; out[2i + {0, 1}] = digits of the product.
+// ===========================================================================
+
+template <int L>
+__device__ void rows_product_one(uint64_t p, const uint64_t* __restrict__ parts, uint64_t n_rows, uint32_t nparts,
+                                 uint64_t i, uint64_t* d0, uint64_t* d1) {
+    const u128 nn = (u128)p * p;
+    uint32_t n[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) n[k] = k < 4 ? (uint32_t)(nn >> (32 * k)) : 0u;
+    uint32_t x = n[0];                  // n^-1 mod 2^32 by Newton
+    for (int k = 0; k < 5; ++k) x *= 2u - n[0] * x;
+    const uint32_t ninv = 0u - x;
+    Res<L> R2;                          // R^2 mod n by doubling 1 (64L times)
+    set_small<L>(R2, 1);
+    for (int k = 0; k < 64 * L; ++k) dbl_mod<L>(R2, n);
+    Res<L> X;                           // running product, Montgomery form
+    for (uint32_t k = 0; k < nparts; ++k) {
+        const uint64_t* d = parts + (uint64_t)k * 2 * n_rows + 2 * i;
+        const u128 v = (u128)d[1] * p + d[0];
+        Res<L> y;
+#pragma unroll
+        for (int w = 0; w < L; ++w) y.w[w] = w < 4 ? (uint32_t)(v >> (32 * w)) : 0u;
+        y = mont_mul<L>(y, R2, n, ninv);                  // v * R
+        X = k ? mont_mul<L>(X, y, n, ninv) : y;
+    }
+    Res<L> one;
+    set_small<L>(one, 1);
+    Res<L> V = mont_mul<L>(X, one, n, ninv);               // out of Montgomery form
+    reduce_full<L>(V, n);
+    digits_base_p<L>(V, p, d0, d1);
+}
+
+__global__ void __launch_bounds__(128)
+k_rows_product(const uint64_t* __restrict__ ps, uint64_t n_rows, const uint64_t* __restrict__ parts, uint32_t nparts,
+               uint64_t* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rows) return;
+    const uint64_t p = ps[i];
+    uint64_t d0, d1;
+    if (p < (1ull << 31)) rows_product_one<2>(p, parts, n_rows, nparts, i, &d0, &d1);
+    else if (p < (1ull << 47)) rows_product_one<3>(p, parts, n_rows, nparts, i, &d0, &d1);
+    else rows_product_one<4>(p, parts, n_rows, nparts, i, &d0, &d1);
+    out[2 * i] = d0;
+    out[2 * i + 1] = d1;
+}
+
+// ===========================================================================
 // Columns above 2^32.  A window [lo, hi) is sieved by CTAs that each own
 // `spc` consecutive segments of BIG_SPAN integers.  Odd primes 3..61 are
 // removed by OR-ing precomputed 32-bit masks (one table per prime, indexed by
@@ -1848,6 +1901,11 @@ void launch_finish(int L, const Bucket* buckets, const RowInfo* info, const RowM
     if (L == 2) k_finish<2><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
     else if (L == 3) k_finish<3><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
     else k_finish<4><<<g, 128, 0, st>>>(buckets, info, mods, part, defs, K, ipart, row_begin, nrows, full, out, acc1, def1, acc2, def2, acc1 != nullptr);
+}
+void launch_rows_product(const uint64_t* ps, uint64_t n_rows, const uint64_t* parts, uint32_t nparts, uint64_t* out,
+                         cudaStream_t st) {
+    if (!n_rows || !nparts) return;
+    k_rows_product<<<(unsigned)((n_rows + 127) / 128), 128, 0, st>>>(ps, n_rows, parts, nparts, out);
 }
 
 }  // namespace wl

@@ -153,6 +153,17 @@ int wl_rows_from(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_lo, uint6
 int wl_search_from(wl_ctx *ctx, uint64_t pmin, uint64_t pmax, uint64_t q_lo, const uint64_t *init,
                    wl_result *results, size_t cap, wl_stats *stats);
 
+/* Row-wise product of partial column products, for a column interval split
+ * between GPUs (each piece from wl_rows_from with init = NULL; the product is
+ * the init of the finishing wl_search_from).  The reference has one device and
+ * folds work-group partials into a residue with reduce.cl:11-44; this is that
+ * fold across pieces.  parts holds nparts arrays of n rows:
+ * parts[k*2n + 2i] + p[i]*parts[k*2n + 2i + 1] is row i's k-th partial (digits
+ * < p[i], p[i] odd in [5, 2^62)); out[2i] + p[i]*out[2i+1] receives the product
+ * mod p[i]^2.  Computed on the GPU; WL_ERR_ARG for a bad p or digit. */
+int wl_rows_product(wl_ctx *ctx, size_t n, const uint64_t *p, size_t nparts, const uint64_t *parts,
+                    uint64_t *out);
+
 /* Forget the resident column table; the next call sieves it again. */
 void wl_drop_columns(wl_ctx *ctx);
 

@@ -14,6 +14,11 @@ Workloads (--workload):
                 rows, 1.3e14 column cells, hours per step), column sweep capped at
                 q < 2^28.  One wl_batch call per step; the same ranges as a loop of
                 per-range wl_search calls (the plain form) are timed beside it.
+  column-shard  the plain-small range [1e9, 1e9 + 1e6), full search, with its
+                column interval split over the ranks (strong scaling): each rank
+                computes its piece's per-row partial products, rank 0 gathers
+                them (16 B per row and rank), multiplies them row-wise on its GPU
+                and finishes (tail, lift, results, checksum).
   serving       a Poisson stream of --requests range requests (default 256) from
                 numpy default_rng(1): exponential inter-arrival times at --rate
                 requests/s, log-uniform starts in [1e8, 2^62-1e7), widths
@@ -92,6 +97,9 @@ def workload(name: str, rank: int, world: int, width: int = 0, qcap: int = -1, m
         q = 0 if qcap < 0 else qcap
         a = PLAIN_SMALL[0] + rank * w
         return [(a, a + w)], q, f"plain-small: every prime in [{a}, {a + w}), " + ("full search" if not q else f"columns q < {q}")
+    if name == "column-shard":
+        a, w = PLAIN_SMALL[0], width or PLAIN_SMALL[1]
+        return [(a, a + w)], 0, f"column-shard: every prime in [{a}, {a + w}), full search, columns split over {world} ranks"
     if name == "plain-mid":
         w = width or 10**7
         q = 2**32 if qcap < 0 else qcap
@@ -339,6 +347,106 @@ def run_serving(args, rank, world, local):
     return 0
 
 
+def run_column_shard(args, rank, world, local):
+    """One range, its columns split over the ranks (clwilson_b200.colshard).
+    Each step re-sieves the columns; rank 0's events span its piece, the
+    gather and the finish, so the step time is the max over ranks."""
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import clwilson_b200 as wl
+    from clwilson_b200 import colshard
+    eng = wl.Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+    (lo, hi), = workload("column-shard", rank, world, args.width)[0]
+    bounds = colshard.column_pieces(lo, hi, world)
+    peak_mad = wl.probe("mad", local)
+    L = limbs_for(hi - 1)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MiB > L2
+
+    def step():
+        eng.drop_columns()
+        part, st = None, None
+        if rank < len(bounds) - 1:
+            part, st = eng.rows_from(lo, hi, bounds[rank], bounds[rank + 1])
+        parts = [part] if world == 1 else colshard.gather_to_rank0(part, rank, world)
+        res = colshard.finish_pieces(eng, lo, hi, bounds, parts) if rank == 0 else None
+        return st, res
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    dev_ms, wall_s, out = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.add_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t0 = time.perf_counter()
+            st, res = step()
+            t1 = time.perf_counter()
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms.append(e0.elapsed_time(e1))
+            wall_s.append(t1 - t0)
+            out.append((st, res))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    pieces = [st for st, _ in out if st is not None]
+    fins = [res for _, res in out if res is not None]
+    tested = sum(r.stats.tested for r in fins)
+    cells = sum(s.cells for s in pieces)
+    sweep_s = sum(s.ms_sweep for s in pieces) / 1e3
+    # the piece calls, the row-wise product (one kernel) and the finishing calls
+    launches = sum(s.kernel_launches for s in pieces) + sum(r.stats.kernel_launches + 1 for r in fins)
+    h2d = (pieces[-1].h2d_bytes if pieces else 0) + (fins[-1].stats.h2d_bytes if fins else 0)
+    d2h = (pieces[-1].d2h_bytes if pieces else 0) + (fins[-1].stats.d2h_bytes if fins else 0)
+    (tot_dev, tot_wall, _), (tested_all, cells_all, launches_all) = merge_over_ranks(
+        dist, [sum(dev_ms) / 1e3, sum(wall_s), sweep_s], [tested, cells, launches])
+    achieved = cells * OPS_PER_CELL[L] / max(sweep_s, 1e-9) / 1e12
+    line = {
+        "metric": "primes tested/s", "value": tested_all / tot_dev, "unit": "primes/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_dev / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"column-shard: every prime in [{lo}, {hi}), full search, columns split over "
+                               f"{world} ranks", "column_bounds": bounds, "limbs": L,
+                   "test_primes_per_step": tested_all / args.steps,
+                   "column_mulmods_per_step": cells_all / args.steps,
+                   "l2": "256 MiB buffer written between steps", "columns": "re-sieved every step",
+                   "parallelism": f"columns sharded, {world} pieces; one gather of 16 B per row and rank to rank 0"},
+        "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_mad / 1e12, "unit": "TOP/s",
+                     "frac": achieved * 1e12 / peak_mad, "traffic": None, "kernel": f"k_sweep<{L},*> (rank {rank})",
+                     "ops_per_cell": OPS_PER_CELL[L],
+                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
+        "e2e": {"value": tested_all / tot_wall, "unit": "primes/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches_all),
+        "tuning": "defaults",
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        one = eng.search(lo, hi)
+        line["checksum_equal_one_call"] = all(r.checksum == one.checksum and r.results == one.results for r in fins)
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"], _, _ = cpu_baseline(lo, hi, 0)
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,7 +454,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain-small",
-                    choices=["plain-small", "plain-mid", "plain-top", "batched", "serving"])
+                    choices=["plain-small", "plain-mid", "plain-top", "batched", "serving", "column-shard"])
     ap.add_argument("--max-width", type=int, default=2000,
                     help="batched/serving: truncate each range to this many integers (0: whole ranges)")
     ap.add_argument("--requests", type=int, default=256, help="serving: requests in the stream")
@@ -369,6 +477,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "serving":
         return run_serving(args, rank, world, local)
+    if args.workload == "column-shard":
+        return run_column_shard(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)

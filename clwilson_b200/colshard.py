@@ -105,7 +105,9 @@ def finish_pieces(engine, pmin: int, pmax: int, bounds: Sequence[int], parts: Se
     return engine.search_from(pmin, pmax, bounds[-1], init=init)
 
 
-def _gather_to_rank0(obj, rank: int, world: int, group=None):
+def gather_to_rank0(obj, rank: int, world: int, group=None):
+    """One object per rank, in rank order, on rank 0 (None elsewhere):
+    torch.distributed.gather_object over `group`."""
     import torch.distributed as dist
     out = [None] * world if rank == 0 else None
     dist.gather_object(obj, out, dst=0, group=group)
@@ -127,7 +129,7 @@ def search_columns_sharded(engine, pmin: int, pmax: int, rank: int = 0, world: i
     elif gather is not None:
         parts = gather(part)
     else:
-        parts = _gather_to_rank0(part, rank, world, group)
+        parts = gather_to_rank0(part, rank, world, group)
     if rank != 0:
         return None
     return finish_pieces(engine, pmin, pmax, bounds, parts)

@@ -62,18 +62,34 @@ def modelled_cells(pmin: int, q: float) -> float:
     return sum(w * _li(min(q, (pmin - 1) / k)) for w, k in zip(CLASS_SHARE, CLASS_DIV))
 
 
-def column_pieces(pmin: int, pmax: int, world: int) -> List[int]:
+def finish_cells(pmin: int, pmax: int) -> float:
+    """Modelled cost of rank 0's finish per test prime, in cells: the
+    consecutive-integer tail T_type+1 .. T_p of each row (iterate.cl), on
+    average (pmax - pmin) / (2k) integers for class divisor k.  The finish
+    also has a fixed cost (about 6.5 ms on B200: test primes, row setup, the
+    row-wise product, the lift); it is left out of the model, which counts
+    cells and not the column sieve, and would overrate it for ranges with
+    few test primes."""
+    width = pmax - pmin
+    return sum(w * width / (2.0 * k) for w, k in zip(CLASS_SHARE, CLASS_DIV))
+
+
+def column_pieces(pmin: int, pmax: int, world: int, rank0_extra: Optional[float] = None) -> List[int]:
     """Boundaries 2 = b_0 < b_1 < ... < b_m = column_end(pmax) of m <= world
-    pieces [b_r, b_{r+1}) with about equal modelled cells.  m < world only
-    when there are fewer columns than ranks."""
+    pieces [b_r, b_{r+1}).  Rank 0 also finishes the search, so its piece plus
+    `rank0_extra` (cells per test prime; default finish_cells) and every other
+    piece have about equal modelled cells.  m < world only when there are
+    fewer columns than ranks."""
     if world < 1:
         raise ValueError("world must be >= 1")
     q_end = column_end(pmax)
     m = max(1, min(world, q_end - 2))
     total = modelled_cells(pmin, q_end)
+    extra = 0.0 if m == 1 else (finish_cells(pmin, pmax) if rank0_extra is None else rank0_extra)
+    each = (total + extra) / m
     bounds = [2]
     for r in range(1, m):
-        goal = total * r / m
+        goal = max(0.0, each * r - extra)
         lo, hi = bounds[-1] + 1, q_end - (m - r)
         # the first integer x in [lo, hi] with modelled_cells(x) >= goal
         a, b = lo, hi

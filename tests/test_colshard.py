@@ -1,7 +1,8 @@
 """Column sharding (clwilson_b200.colshard) on CPU.
 
 The planner: boundaries strictly increase from 2 to the first column above
-every class target, with about equal modelled cells per piece.
+every class target, with about equal modelled cells per piece once rank 0's
+piece is charged the tail it also runs.
 
 The flow: gloo ranks (world sizes 2 and 3) run search_columns_sharded with
 an engine whose calls are answered by the oracle.  The pieces are products
@@ -41,7 +42,16 @@ def test_pieces_balanced(pmin, pmax, world):
     assert len(b) == world + 1 and b[0] == 2 and b[-1] == colshard.column_end(pmax)
     assert all(x < y for x, y in zip(b, b[1:]))
     w = [colshard.modelled_cells(pmin, y) - colshard.modelled_cells(pmin, x) for x, y in zip(b, b[1:])]
+    # rank 0 also runs the tail of every row: its piece is smaller by that
+    extra = colshard.finish_cells(pmin, pmax)
+    if extra > 1.0:
+        assert w[0] < w[1]
+    w[0] += extra
     assert max(w) <= 1.01 * min(w)
+    # without the discount all pieces are equal
+    b2 = colshard.column_pieces(pmin, pmax, world, rank0_extra=0.0)
+    w2 = [colshard.modelled_cells(pmin, y) - colshard.modelled_cells(pmin, x) for x, y in zip(b2, b2[1:])]
+    assert max(w2) <= 1.01 * min(w2)
 
 
 def test_pieces_tiny_ranges():

@@ -5,6 +5,8 @@ and serving: ranges / requests round-robin) with no data-path collective; the
 only collectives are the barrier and the whole-job reduction (max of timings,
 sum of work).  Checked here: the shards are disjoint and cover the
 configuration, and the reduction gives the max and the sum on every rank.
+The column-shard workload gives every rank the same range instead; its
+columns are split and gathered as tests/test_colshard.py checks.
 """
 import os
 import socket
@@ -29,7 +31,7 @@ def _rank_main(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         shards = {}
-        for name in ("plain-small", "plain-mid", "plain-top", "batched"):
+        for name in ("plain-small", "plain-mid", "plain-top", "batched", "column-shard"):
             ranges, qcap, _ = bench.workload(name, rank, world)
             shards[name] = (ranges, qcap)
         reqs = bench.serving_requests(1, 32, 64.0, 2000)[rank::world]
@@ -60,6 +62,8 @@ def test_two_ranks_shard_and_reduce():
         (x1, y1), = s1[name][0]
         assert y0 <= x1 or y1 <= x0, name
         assert s0[name][1] == s1[name][1] == 2**32
+    # column-shard: every rank holds the whole range, full search (its columns are split)
+    assert s0["column-shard"] == s1["column-shard"] == ([(10**9, 10**9 + 10**6)], 0)
     # batched: the 256 ranges split round-robin, nothing lost or repeated
     import bench
     allr = bench.batched_ranges(0, max_width=2000)

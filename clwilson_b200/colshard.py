@@ -4,7 +4,8 @@ The reference runs a range on one device.  It sweeps the columns (sieving
 primes q <= T, the class target) chunk by chunk and folds each chunk's
 work-group partial products into the residues (cl_wilson.cpp:1856-1929,
 reduce.cl:11-44).  Here the column interval [2, q_end) of one range is cut
-into one piece per rank, at boundaries that balance the modelled cell count.
+into one piece per rank, at boundaries that balance the modelled work (cells
+and column sieve; rank 0 is charged the finish it also runs).
 
 * Each rank computes its piece's per-row partial products with
   wl_rows_from, starting from 1.
@@ -30,6 +31,16 @@ from typing import Callable, List, Optional, Sequence
 CLASS_SHARE = (0.5, 0.25, 0.25)
 # class target T = (p - 1) / k per class (cl_wilson.cpp:1549-1586)
 CLASS_DIV = (6, 4, 2)
+# ranges up to this width are planned from their actual test primes
+EXACT_PLAN_WIDTH = 1 << 14
+
+# Costs in cells of the sparse sweep (about 1.4e12 cells/s on B200):
+# sieving the columns costs about 1.1e-12 s per integer below and above 2^32
+# (the resident column sieve; the windowed sieve with its bitmap sweep), and
+# the finishing call about 6.5 ms besides its tail (test primes, row setup,
+# the row-wise product, the lift), both measured on B200.
+SIEVE_CELLS_PER_INTEGER = 1.6
+FINISH_FIXED_CELLS = 9.0e9
 
 
 def column_end(pmax: int) -> int:
@@ -37,6 +48,83 @@ def column_end(pmax: int) -> int:
 
     The largest target is (p - 1) / 2 of a class-2 prime p < pmax."""
     return (pmax - 2) // 2 + 1
+
+
+def _is_prime(n: int) -> bool:
+    """Miller-Rabin with the first 12 prime bases (exact below 3.3e24)."""
+    if n < 2:
+        return False
+    small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+    for q in small:
+        if n % q == 0:
+            return n == q
+    d, r = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        r += 1
+    for a in small:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(r - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def _class_of(p: int) -> int:
+    return 0 if p % 3 == 1 else (1 if p % 12 == 5 else 2)
+
+
+class RangeModel:
+    """What the planner knows of a range: the number of test primes, each
+    class's share of them and its shared target (the target of the class's
+    first prime).  Exact for ranges up to EXACT_PLAN_WIDTH integers (host
+    primality test; planning only, the engine finds the primes itself),
+    otherwise the asymptotic shares with targets (pmin - 1) / k."""
+
+    def __init__(self, pmin: int, pmax: int):
+        self.pmin, self.pmax = pmin, pmax
+        if pmax - pmin <= EXACT_PLAN_WIDTH:
+            first = [0, 0, 0]
+            count = [0, 0, 0]
+            for p in range(max(pmin, 5), pmax):
+                if _is_prime(p):
+                    t = _class_of(p)
+                    if not count[t]:
+                        first[t] = p
+                    count[t] += 1
+            n = sum(count)
+            self.rows = float(max(n, 1))
+            self.share = tuple(c / max(n, 1) for c in count)
+            self.targets = tuple((first[t] - 1) // CLASS_DIV[t] if count[t] else 0 for t in range(3))
+        else:
+            self.rows = max(1.0, (pmax - pmin) / math.log(max(pmin, 3)))
+            self.share = CLASS_SHARE
+            self.targets = tuple((pmin - 1) / k for k in CLASS_DIV)
+
+    def cells(self, q: float) -> float:
+        """Modelled cells per test prime of the columns below q: each class
+        sweeps about li(min(q, T)) primes, weighted by its share."""
+        return sum(w * _li(min(q, T)) for w, T in zip(self.share, self.targets) if w)
+
+    def work(self, q: float) -> float:
+        """Modelled cost of the columns below q, in cells: every test prime's
+        cells plus the sieve of the integers up to the largest target."""
+        sieved = max(0.0, min(q, max(self.targets)) - 2)
+        return self.rows * self.cells(q) + SIEVE_CELLS_PER_INTEGER * sieved
+
+    def finish(self) -> float:
+        """Modelled cost of rank 0's finish, in cells: the consecutive-integer
+        tail T_type+1 .. T_p of each row (iterate.cl), on average
+        (pmax - pmin) / (2k) integers for class divisor k, plus the call's
+        fixed cost."""
+        width = self.pmax - self.pmin
+        tail = sum(w * width / (2.0 * k) for w, k in zip(self.share, CLASS_DIV))
+        return self.rows * tail + FINISH_FIXED_CELLS
 
 
 def _li(x: float) -> float:
@@ -54,48 +142,34 @@ def _li(x: float) -> float:
     return s * h / 3
 
 
-def modelled_cells(pmin: int, q: float) -> float:
-    """Modelled cells of the columns below q, per test prime of the range.
-
-    Each class sweeps the primes up to its target, about li(min(q, T)) of
-    them, weighted by its share of the test primes."""
-    return sum(w * _li(min(q, (pmin - 1) / k)) for w, k in zip(CLASS_SHARE, CLASS_DIV))
-
-
-def finish_cells(pmin: int, pmax: int) -> float:
-    """Modelled cost of rank 0's finish per test prime, in cells: the
-    consecutive-integer tail T_type+1 .. T_p of each row (iterate.cl), on
-    average (pmax - pmin) / (2k) integers for class divisor k.  The finish
-    also has a fixed cost (about 6.5 ms on B200: test primes, row setup, the
-    row-wise product, the lift); it is left out of the model, which counts
-    cells and not the column sieve, and would overrate it for ranges with
-    few test primes."""
-    width = pmax - pmin
-    return sum(w * width / (2.0 * k) for w, k in zip(CLASS_SHARE, CLASS_DIV))
-
-
-def column_pieces(pmin: int, pmax: int, world: int, rank0_extra: Optional[float] = None) -> List[int]:
+def column_pieces(pmin: int, pmax: int, world: int, rank0_extra: Optional[float] = None,
+                  model: Optional[RangeModel] = None) -> List[int]:
     """Boundaries 2 = b_0 < b_1 < ... < b_m = column_end(pmax) of m <= world
     pieces [b_r, b_{r+1}).  Rank 0 also finishes the search, so its piece plus
-    `rank0_extra` (cells per test prime; default finish_cells) and every other
-    piece have about equal modelled cells.  m < world only when there are
-    fewer columns than ranks."""
+    `rank0_extra` (cells; default the model's finish) and every other piece
+    have about equal modelled work; when the finish alone outweighs a piece,
+    rank 0's piece is one column.  m < world only when there are fewer
+    columns than ranks."""
     if world < 1:
         raise ValueError("world must be >= 1")
+    model = model or RangeModel(pmin, pmax)
     q_end = column_end(pmax)
     m = max(1, min(world, q_end - 2))
-    total = modelled_cells(pmin, q_end)
-    extra = 0.0 if m == 1 else (finish_cells(pmin, pmax) if rank0_extra is None else rank0_extra)
-    each = (total + extra) / m
+    total = model.work(q_end)
+    extra = 0.0 if m == 1 else (model.finish() if rank0_extra is None else rank0_extra)
+    # rank 0's share; when the finish alone outweighs a piece, rank 0 keeps
+    # one column and the other ranks share the rest equally
+    first = max(0.0, (total + extra) / m - extra)
+    other = (total - first) / (m - 1) if m > 1 else total
     bounds = [2]
     for r in range(1, m):
-        goal = max(0.0, each * r - extra)
+        goal = first + other * (r - 1)
         lo, hi = bounds[-1] + 1, q_end - (m - r)
-        # the first integer x in [lo, hi] with modelled_cells(x) >= goal
+        # the first integer x in [lo, hi] with work(x) >= goal
         a, b = lo, hi
         while a < b:
             mid = (a + b) // 2
-            if modelled_cells(pmin, mid) >= goal:
+            if model.work(mid) >= goal:
                 b = mid
             else:
                 a = mid + 1

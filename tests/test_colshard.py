@@ -1,8 +1,9 @@
 """Column sharding (clwilson_b200.colshard) on CPU.
 
 The planner: boundaries strictly increase from 2 to the first column above
-every class target, with about equal modelled cells per piece once rank 0's
-piece is charged the tail it also runs.
+every class target, with about equal modelled work per piece once rank 0's
+piece is charged the finish it also runs; the range model of narrow ranges
+has the oracle's class counts and targets.
 
 The flow: gloo ranks (world sizes 2 and 3) run search_columns_sharded with
 an engine whose calls are answered by the oracle.  The pieces are products
@@ -34,24 +35,48 @@ def test_column_end_covers_every_target():
         assert end <= pmax // 2 + 1
 
 
-@pytest.mark.parametrize("pmin,pmax,world", [(10**6, 10**6 + 3000, 2), (10**9, 10**9 + 10**6, 8),
+@pytest.mark.parametrize("pmin,pmax,world", [(10**6, 10**6 + 3000, 2), (10**6, 10**6 + 3000, 5),
+                                             (10**9, 10**9 + 10**6, 8),
                                              (1239053554603, 1239053554604, 4), ((1 << 62) - 10**6, (1 << 62) - 1, 8),
                                              (10**13, 10**13 + 10**6, 3)])
 def test_pieces_balanced(pmin, pmax, world):
-    b = colshard.column_pieces(pmin, pmax, world)
+    m = colshard.RangeModel(pmin, pmax)
+    b = colshard.column_pieces(pmin, pmax, world, model=m)
     assert len(b) == world + 1 and b[0] == 2 and b[-1] == colshard.column_end(pmax)
     assert all(x < y for x, y in zip(b, b[1:]))
-    w = [colshard.modelled_cells(pmin, y) - colshard.modelled_cells(pmin, x) for x, y in zip(b, b[1:])]
-    # rank 0 also runs the tail of every row: its piece is smaller by that
-    extra = colshard.finish_cells(pmin, pmax)
-    if extra > 1.0:
-        assert w[0] < w[1]
-    w[0] += extra
+    w = [m.work(y) - m.work(x) for x, y in zip(b, b[1:])]
+    # rank 0 also runs the finish: its piece is smaller by the modelled finish,
+    # or one column when the finish outweighs a whole piece
+    assert w[0] < w[1]
+    if m.finish() < m.work(b[-1]) / world:
+        w[0] += m.finish()
+    else:
+        assert b[1] == 3
+        w = w[1:]
     assert max(w) <= 1.01 * min(w)
     # without the discount all pieces are equal
-    b2 = colshard.column_pieces(pmin, pmax, world, rank0_extra=0.0)
-    w2 = [colshard.modelled_cells(pmin, y) - colshard.modelled_cells(pmin, x) for x, y in zip(b2, b2[1:])]
+    b2 = colshard.column_pieces(pmin, pmax, world, rank0_extra=0.0, model=m)
+    w2 = [m.work(y) - m.work(x) for x, y in zip(b2, b2[1:])]
     assert max(w2) <= 1.01 * min(w2)
+
+
+def test_range_model_exact_for_narrow_ranges():
+    # class counts and shared targets as the oracle finds them
+    for pmin, pmax in [(200, 564), (10**6, 10**6 + 3000), (2**31 - 1000, 2**31 + 1000), (10**12, 10**12 + 5000)]:
+        m = colshard.RangeModel(pmin, pmax)
+        rows, targets = oracle.search(pmin, pmax, qcap=2)
+        assert m.rows == len(rows)
+        assert list(m.targets) == [int(t) for t in targets]
+        counts = np.bincount(rows["type"].astype(np.int64), minlength=3)
+        assert np.allclose(np.array(m.share) * len(rows), counts)
+    # self-test case 1: one class-0 prime; every boundary but the end lies below its target
+    m = colshard.RangeModel(1239053554603, 1239053554604)
+    assert m.rows == 1 and m.share == (1.0, 0.0, 0.0) and m.targets == ((1239053554603 - 1) // 6, 0, 0)
+    b = colshard.column_pieces(1239053554603, 1239053554604, 3, model=m)
+    assert all(x < m.targets[0] for x in b[:-1])
+    # wide ranges: asymptotic shares, targets (pmin - 1) / k
+    m = colshard.RangeModel(10**9, 10**9 + 10**6)
+    assert m.share == colshard.CLASS_SHARE and abs(m.rows - 10**6 / np.log(10**9)) < 1
 
 
 def test_pieces_tiny_ranges():

@@ -374,8 +374,8 @@ def run_column_shard(args, rank, world, local):
         part, st = None, None
         if rank < len(bounds) - 1:
             part, st = eng.rows_from(lo, hi, bounds[rank], bounds[rank + 1])
-        parts = [part] if world == 1 else colshard.gather_to_rank0(part, rank, world)
-        res = colshard.finish_pieces(eng, lo, hi, bounds, parts) if rank == 0 else None
+        parts = [part] if world == 1 else colshard.gather_to_rank0(colshard.piece_digits(part), rank, world)
+        res = colshard.finish_pieces(eng, lo, hi, bounds, parts, p=part["p"]) if rank == 0 else None
         return st, res
 
     for _ in range(args.warmup):

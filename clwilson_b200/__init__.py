@@ -392,24 +392,35 @@ class Engine:
         out = [(res[i].p, res[i].value) for i in range(min(st.results, cap))]
         return SearchResult(out, st.checksum, Stats.from_c(st))
 
-    def rows_product(self, parts) -> np.ndarray:
+    def rows_product(self, parts, p=None) -> np.ndarray:
         """Row-wise product of partial column products (wl_rows_product).
 
-        `parts`: row arrays of one range (wl_rows_from pieces over disjoint
-        column intervals, same primes in the same order).  Returns rows with
-        p and the digits (s0, s1) of the product mod p^2, the init of the
-        finishing search_from."""
+        `parts`: pieces of one range over disjoint column intervals (same
+        primes, same order), each either rows (wl_rows_from) or an (n, 2)
+        array of digits (s0, s1).  `p`: the primes, when no part is rows.
+        Returns rows with p and the digits (s0, s1) of the product mod p^2,
+        the init of the finishing search_from."""
         parts = list(parts)
         if not parts:
             raise ValueError("rows_product needs at least one part")
-        p = np.ascontiguousarray(parts[0]["p"], dtype=np.uint64)
-        for x in parts[1:]:
-            if not np.array_equal(x["p"], p):
-                raise ValueError("rows_product: the parts hold different primes")
+        rows_parts = [x for x in parts if x.dtype.names]
+        if p is None:
+            if not rows_parts:
+                raise ValueError("rows_product: give p or at least one part as rows")
+            p = rows_parts[0]["p"]
+        p = np.ascontiguousarray(p, dtype=np.uint64)
         n = p.size
-        digits = np.ascontiguousarray(
-            np.stack([np.stack([np.asarray(x["s0"], dtype=np.uint64), np.asarray(x["s1"], dtype=np.uint64)], axis=1)
-                      for x in parts]))
+        digits = np.empty((len(parts), n, 2), dtype=np.uint64)
+        for k, x in enumerate(parts):
+            if x.dtype.names:
+                if not np.array_equal(x["p"], p):
+                    raise ValueError("rows_product: the parts hold different primes")
+                digits[k, :, 0] = x["s0"]
+                digits[k, :, 1] = x["s1"]
+            else:
+                if x.shape != (n, 2):
+                    raise ValueError("rows_product: a digit part must have shape (%d, 2)" % n)
+                digits[k] = x
         out = np.zeros((max(n, 1), 2), dtype=np.uint64)
         rc = self._L.wl_rows_product(self._ctx, n, p.ctypes.data, len(parts), digits.ctypes.data, out.ctypes.data)
         if rc:
@@ -418,7 +429,8 @@ class Engine:
         rows["p"] = p
         rows["s0"] = out[:n, 0]
         rows["s1"] = out[:n, 1]
-        rows["type"] = parts[0]["type"]
+        if rows_parts:
+            rows["type"] = rows_parts[0]["type"]
         return rows
 
     def batch(self, ranges: Sequence[Tuple[int, int]], q_cap: int = 0, cap: int = 1 << 20):

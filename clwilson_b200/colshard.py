@@ -27,6 +27,8 @@ from __future__ import annotations
 import math
 from typing import Callable, List, Optional, Sequence
 
+import numpy as np
+
 # share of test primes per class: p = 1 mod 3, p = 5 mod 12, p = 11 mod 12
 CLASS_SHARE = (0.5, 0.25, 0.25)
 # class target T = (p - 1) / k per class (cl_wilson.cpp:1549-1586)
@@ -186,12 +188,24 @@ def search_piece(engine, pmin: int, pmax: int, bounds: Sequence[int], rank: int)
     return rows
 
 
-def finish_pieces(engine, pmin: int, pmax: int, bounds: Sequence[int], parts: Sequence):
-    """The search result from the pieces of all ranks (in rank order)."""
+def piece_digits(rows):
+    """The digits (s0, s1) of a piece's rows as an (n, 2) uint64 array: the
+    16 bytes per row that cross to rank 0."""
+    if rows is None:
+        return None
+    out = np.empty((rows.size, 2), dtype=np.uint64)
+    out[:, 0] = rows["s0"]
+    out[:, 1] = rows["s1"]
+    return out
+
+
+def finish_pieces(engine, pmin: int, pmax: int, bounds: Sequence[int], parts: Sequence, p=None):
+    """The search result from the pieces of all ranks (in rank order): rows,
+    or digit arrays with the primes `p` (or with one part as rows)."""
     held = [x for x in parts if x is not None]
     if len(held) != len(bounds) - 1:
         raise ValueError("finish_pieces: %d pieces for %d column intervals" % (len(held), len(bounds) - 1))
-    init = engine.rows_product(held)
+    init = engine.rows_product(held, p=p)
     return engine.search_from(pmin, pmax, bounds[-1], init=init)
 
 
@@ -215,11 +229,10 @@ def search_columns_sharded(engine, pmin: int, pmax: int, rank: int = 0, world: i
     bounds = column_pieces(pmin, pmax, world)
     part = search_piece(engine, pmin, pmax, bounds, rank)
     if world == 1:
-        parts = [part]
-    elif gather is not None:
-        parts = gather(part)
-    else:
-        parts = gather_to_rank0(part, rank, world, group)
+        return finish_pieces(engine, pmin, pmax, bounds, [part])
+    mine = piece_digits(part)
+    parts = gather(mine) if gather is not None else gather_to_rank0(mine, rank, world, group)
     if rank != 0:
         return None
-    return finish_pieces(engine, pmin, pmax, bounds, parts)
+    # rank 0 always holds the first piece, whose rows carry the primes
+    return finish_pieces(engine, pmin, pmax, bounds, parts, p=part["p"])

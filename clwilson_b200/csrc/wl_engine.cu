@@ -1068,10 +1068,13 @@ int wl_rows_product(wl_ctx* c, size_t n, const uint64_t* p, size_t nparts, const
     if (!c || nparts == 0 || nparts > (1u << 16) || n > (1ull << 32)) return WL_ERR_ARG;
     if (n == 0) return 0;
     if (!p || !parts || !out) return WL_ERR_ARG;
-    for (size_t i = 0; i < n; ++i) {
+    for (size_t i = 0; i < n; ++i)
         if (p[i] < 5 || p[i] > WL_MAXP || !(p[i] & 1)) return WL_ERR_ARG;
-        for (size_t k = 0; k < nparts; ++k)
-            if (parts[k * 2 * n + 2 * i] >= p[i] || parts[k * 2 * n + 2 * i + 1] >= p[i]) return WL_ERR_ARG;
+    for (size_t k = 0; k < nparts; ++k) {   // part by part, in memory order
+        const uint64_t* d = parts + k * 2 * n;
+        bool bad = false;
+        for (size_t i = 0; i < n; ++i) bad |= (d[2 * i] >= p[i]) | (d[2 * i + 1] >= p[i]);
+        if (bad) return WL_ERR_ARG;
     }
     cudaSetDevice(c->device);
     const size_t pb = n * 8, xb = nparts * n * 16, ob = n * 16;

@@ -110,15 +110,18 @@ class OracleEngine:
             r["s0"], r["s1"] = oracle.range_product(int(r["p"]), targets[int(r["type"])], q_lo, q_cap)
         return rows, None
 
-    def rows_product(self, parts):
-        out = parts[0].copy()
+    def rows_product(self, parts, p=None):
+        # gathered pieces arrive as (n, 2) digit arrays, 16 bytes per row
+        assert p is not None
+        assert all(x.shape == (len(p), 2) and x.dtype == np.uint64 for x in parts)
+        out = np.zeros(len(p), dtype=oracle.ROW_DTYPE)
+        out["p"] = p
         for i in range(out.size):
-            p = int(out["p"][i])
+            q = int(p[i])
             v = 1
             for x in parts:
-                assert int(x["p"][i]) == p
-                v = v * (int(x["s0"][i]) + p * int(x["s1"][i])) % (p * p)
-            out["s0"][i], out["s1"][i] = v % p, v // p
+                v = v * (int(x[i, 0]) + q * int(x[i, 1])) % (q * q)
+            out["s0"][i], out["s1"][i] = v % q, v // q
         return out
 
     def search_from(self, pmin, pmax, q_lo, init=None):

@@ -5,7 +5,8 @@
 * The sharded search must equal the one-call wl_search of the same range:
   pieces from wl_rows_from starting at 1, their row-wise product, then the
   finishing wl_search_from.  Result lines, checksum and the product rows are
-  compared.  Ranges: self-test case 5, rows straddling 2^31, a 20,000-wide
+  compared, with the pieces as rows and as the 16-byte digit arrays ranks
+  exchange.  Ranges: self-test case 5, rows straddling 2^31, a 20,000-wide
   range cut into 8 pieces, and self-test case 1, whose columns reach 2.07e11:
   its pieces start above 2^32 or hold no column of the row at all.
 """
@@ -78,6 +79,11 @@ def test_sharded_matches_one_call(engine, lo, hi, world):
     rows, _ = engine.rows(lo, hi, q_cap=b[-1])      # the product over all columns in one call
     assert np.array_equal(prod["p"], rows["p"])
     assert np.array_equal(prod["s0"], rows["s0"]) and np.array_equal(prod["s1"], rows["s1"])
+    # the pieces as gathered between ranks: 16-byte digit arrays plus the primes
+    parts = [colshard.search_piece(engine, lo, hi, b, r) for r in range(world)]
+    digs = [colshard.piece_digits(x) for x in parts if x is not None]
+    prod2 = engine.rows_product(digs, p=rows["p"])
+    assert np.array_equal(prod2["s0"], rows["s0"]) and np.array_equal(prod2["s1"], rows["s1"])
 
 
 def test_sharded_case5_golden(engine, golden):

@@ -30,7 +30,7 @@ WL_MAXP = 4611686018427387903
 WL_MAX_WIDTH = 10_000_000
 ERRORS = {
     -1: "invalid argument or range", -2: "CUDA error", -3: "there are no primes to test in this range!",
-    -4: "configuration not supported by this build", -5: "Wilson quotient check failed",
+    -4: "configuration not supported by this library", -5: "Wilson quotient check failed",
     -6: "representation a, c or u not found", -7: "result buffer too small", -8: "device allocation failed",
     -9: "request exceeds the fixed scratch of the no-allocation entry point",
 }

@@ -919,7 +919,7 @@ const char* wl_strerror(int code) {
         case WL_ERR_ARG: return "invalid argument or range";
         case WL_ERR_CUDA: return "CUDA error";
         case WL_ERR_NOPRIMES: return "there are no primes to test in this range!";
-        case WL_ERR_UNSUPPORTED: return "configuration not supported by this build";
+        case WL_ERR_UNSUPPORTED: return "configuration not supported by this library";
         case WL_ERR_WILSON_CHECK: return "Wilson quotient check failed";
         case WL_ERR_NO_REPR: return "representation a, c or u not found";
         case WL_ERR_CAPACITY: return "result buffer too small";

@@ -22,6 +22,11 @@
  *   wl_rows               the per-prime residues the reference reads back before
  *                         finalising (getDataFromGPU, cl_wilson.cpp:320-350) plus
  *                         the per-prime quotient of processResult (691-900)
+ *   wl_rows_from /        a search in pieces of columns with checkpoints (the
+ *   wl_search_from        chunked main loop and resume, cl_wilson.cpp:1742-1776,
+ *                         1856-1929)
+ *   wl_rows_product       the fold of partial products into residues
+ *                         (reduce.cl:11-44) across the column pieces of GPUs
  *   wl_batch              many ranges in one device pass (no counterpart: the
  *                         reference runs one range per process)
  *   wl_server_*           a resident serving session with continuous batching
@@ -48,7 +53,7 @@ extern "C" {
 #define WL_ERR_ARG          (-1)   /* bad argument / range rule violated */
 #define WL_ERR_CUDA         (-2)   /* CUDA runtime error */
 #define WL_ERR_NOPRIMES     (-3)   /* no primes in the range (cl_wilson.cpp:1532-1536) */
-#define WL_ERR_UNSUPPORTED  (-4)   /* configuration not supported by this build */
+#define WL_ERR_UNSUPPORTED  (-4)   /* configuration not supported by this library */
 #define WL_ERR_WILSON_CHECK (-5)   /* rem != 0 after the lift (cl_wilson.cpp:866-870) */
 #define WL_ERR_NO_REPR      (-6)   /* a, c or u not found (cl_wilson.cpp:554-558) */
 #define WL_ERR_CAPACITY     (-7)   /* caller buffer too small; *_needed tells the size */

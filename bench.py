@@ -250,7 +250,8 @@ def run_reference(args, rank, world):
     line = {
         "metric": metric, "value": value, "unit": unit, "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "strong" if args.workload == "column-shard" else "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": desc, "sample_rows_per_step": len(sel), "rows_in_workload": n},
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": f"{len(sel)} of {n} primes per step, evenly spaced, q_cap={q_cap}"},

@@ -2,7 +2,8 @@
 //
 // One search (or a batch of ranges) runs as:
 //   1. test primes: deterministic Miller-Rabin over each window [pmin, pmax)
-//      into an ordered list on the device (k_window_primes, k_compact);
+//      into an ordered list on the device (k_window_primes_multi, k_compact), all
+//      ranges in one launch each;
 //   2. classification into (range, class) buckets with the reference's shared
 //      class target = the target of the first prime of the class
 //      (cl_wilson.cpp:1549-1586);
@@ -311,8 +312,9 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
 }
 
 // Test primes of each range, ascending, by deterministic Miller-Rabin over
-// the range's window (k_window_primes, k_compact); rs[i] gets the range's
-// window layout and its offset and count in tps.
+// the range's window (k_window_primes_multi, k_compact: one launch each for
+// all ranges); rs[i] gets the range's window layout and its offset and count
+// in tps.
 int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<RangeState>& rs,
                     std::vector<uint64_t>& tps, bool allow_empty) {
     rs.assign(nr, RangeState());
@@ -331,13 +333,23 @@ int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<Ra
     RC(ensure(c->bitmap, std::max<uint64_t>(words * 4, c->bitmap.cap)));
     RC(ensure(c->segcount, std::max<uint64_t>(segs * 4, c->segcount.cap)));
     RC(ensure(c->offsets, std::max<uint64_t>((segs + 1) * 8, c->offsets.cap)));
-    CK(cudaMemsetAsync(c->segcount.p, 0, segs * 4, c->st));
+    // every range in one launch, each over its own integers only (512 per block)
+    std::vector<WinDesc> wd(nr);
+    uint64_t blocks = 0;
     for (size_t i = 0; i < nr; ++i) {
-        RangeState& r = rs[i];
-        launch_window_primes(r.lo0, r.pmin, r.pmax, r.nseg, as<uint32_t>(c->bitmap) + r.word_off,
-                             as<uint32_t>(c->segcount) + r.seg_off, c->st);
-        c->launches++;
+        const RangeState& r = rs[i];
+        wd[i] = WinDesc{ r.lo0, r.pmin, r.pmax, r.word_off, r.seg_off, (uint32_t)blocks, 0 };
+        blocks += (r.pmax - r.lo0 + 511) / 512;
     }
+    if (blocks >= (1ull << 31)) return WL_ERR_UNSUPPORTED;
+    RC(ensure(c->windesc, nr * sizeof(WinDesc)));
+    CK(cudaMemcpyAsync(c->windesc.p, wd.data(), nr * sizeof(WinDesc), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->bitmap.p, 0, words * 4, c->st));
+    CK(cudaMemsetAsync(c->segcount.p, 0, segs * 4, c->st));
+    launch_window_primes_multi(as<WinDesc>(c->windesc), (uint32_t)nr, (uint32_t)blocks, as<uint32_t>(c->bitmap),
+                               as<uint32_t>(c->segcount), c->st);
+    c->launches++;
+    c->h2d += nr * sizeof(WinDesc);
     std::vector<uint32_t> segcnt(segs);
     CK(cudaMemcpyAsync(segcnt.data(), c->segcount.p, segs * 4, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -358,14 +370,17 @@ int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<Ra
     offs[segs] = total;
     if (total >= (1ull << 31)) return WL_ERR_UNSUPPORTED;
     RC(ensure(c->tp, total * 8));
+    std::vector<uint64_t> seg_lo(segs);
+    for (size_t i = 0; i < nr; ++i)
+        for (uint32_t s = 0; s < rs[i].nseg; ++s) seg_lo[rs[i].seg_off + s] = rs[i].lo0 + (uint64_t)s * SEG_SPAN;
+    RC(ensure(c->seglo, segs * 8));
     CK(cudaMemcpyAsync(c->offsets.p, offs.data(), (segs + 1) * 8, cudaMemcpyHostToDevice, c->st));
-    c->h2d += (segs + 1) * 8;
-    for (size_t i = 0; i < nr; ++i) {
-        RangeState& r = rs[i];
-        launch_compact(r.nseg, r.lo0, as<uint32_t>(c->bitmap) + r.word_off, as<uint64_t>(c->offsets) + r.seg_off,
-                       nullptr, as<uint64_t>(c->tp), c->st);
-        c->launches++;
-    }
+    CK(cudaMemcpyAsync(c->seglo.p, seg_lo.data(), segs * 8, cudaMemcpyHostToDevice, c->st));
+    c->h2d += (segs + 1) * 8 + segs * 8;
+    // every range's segments in one ordered write-out
+    launch_compact_multi((uint32_t)segs, as<uint64_t>(c->seglo), as<uint32_t>(c->bitmap), as<uint64_t>(c->offsets),
+                         as<uint64_t>(c->tp), c->st);
+    c->launches++;
     tps.assign(total, 0);
     CK(cudaMemcpyAsync(tps.data(), c->tp.p, total * 8, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -986,7 +1001,7 @@ void wl_close(wl_ctx* c) {
                        &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
                        &c->bbitmap, &c->bsegcount, &c->boffsets, &c->boffs, &c->wcols, &c->wbuckets, &c->witems,
                        &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts, &c->uacc, &c->udef,
-                       &c->defs, &c->rowout, &c->prod };
+                       &c->defs, &c->rowout, &c->prod, &c->windesc, &c->seglo };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->fork) cudaEventDestroy(c->fork);

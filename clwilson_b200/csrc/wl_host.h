@@ -86,6 +86,7 @@ struct wl_ctx {
     DevBuf bbitmap, bsegcount, boffsets, boffs, wcols, wbuckets, witems, wpart, wdefs, bacc, bdef, wkeys, wcounts;
     DevBuf uacc, udef;   // columns below 2^32: per-row product of all splits, per-bucket deficit
     DevBuf prod;         // wl_rows_product: moduli, partial products, products
+    DevBuf windesc, seglo;   // test-prime windows of all ranges, their segment starts
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;

@@ -118,8 +118,17 @@ void launch_scan_counts(const uint32_t* counts, uint32_t n, uint64_t first, uint
                         cudaStream_t st);
 void launch_compact(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets,
                     uint32_t* out32, uint64_t* out64, cudaStream_t st);
-void launch_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t* bitmap,
-                          uint32_t* seg_count, cudaStream_t st);
+// One range's window of test primes: odd numbers lo0 + 2i + 1 tested in [lo, hi);
+// bitmap words from word_off, segment counts from seg_off, blocks from block0.
+struct WinDesc {
+    uint64_t lo0, lo, hi;
+    uint64_t word_off, seg_off;
+    uint32_t block0, pad;
+};
+void launch_window_primes_multi(const WinDesc* d, uint32_t nr, uint32_t nblocks, uint32_t* bitmap,
+                                uint32_t* seg_count, cudaStream_t st);
+void launch_compact_multi(uint32_t nseg, const uint64_t* seg_lo, const uint32_t* bitmap, const uint64_t* offsets,
+                          uint64_t* out64, cudaStream_t st);
 void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys,
                       uint64_t* out, cudaStream_t st);
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);

@@ -1,7 +1,7 @@
 // wl_kernels.cu -- sm_100a kernels of the Wilson-prime engine.
 //
 //   k_sieve_segments / k_compact   sieving primes q < 2^32 (the columns)
-//   k_window_primes                test primes in [pmin, pmax) (the rows)
+//   k_window_primes_multi          test primes in [pmin, pmax) of every range (the rows)
 //   k_setup_rows                   per-row modulus constants (setup.cl)
 //   k_sweep<L,RPT>                 prod_{q <= T} q^{v_q(T!)} over a column split
 //                                  (mulsmall.cl / mullarge.cl / reduce.cl)
@@ -107,11 +107,12 @@ k_scan_counts(const uint32_t* __restrict__ counts, uint32_t n, uint64_t first, u
 }
 
 // Ordered write-out of the numbers whose bit is set: segment s covers odd
-// numbers lo0 + s*span + 2i + 1.  Writes 32-bit or 64-bit values.
+// numbers lo + 2i + 1 with lo = seg_lo[s], or lo0 + s*span without seg_lo.
+// Writes 32-bit or 64-bit values.
 constexpr uint32_t COMPACT_THREADS = 256;
 __global__ void __launch_bounds__(COMPACT_THREADS)
 k_compact(uint64_t lo0, uint32_t span, const uint32_t* __restrict__ bitmap, const uint64_t* __restrict__ offsets,
-          uint32_t* __restrict__ out32, uint64_t* __restrict__ out64) {
+          uint32_t* __restrict__ out32, uint64_t* __restrict__ out64, const uint64_t* __restrict__ seg_lo) {
     __shared__ uint32_t wsum[COMPACT_THREADS / 32];
     constexpr uint32_t WPT = SEG_WORDS / COMPACT_THREADS;   // words per thread
     const uint32_t seg = blockIdx.x;
@@ -132,7 +133,7 @@ k_compact(uint64_t lo0, uint32_t span, const uint32_t* __restrict__ bitmap, cons
     uint32_t wbase = 0;
     for (uint32_t i = 0; i < wid; ++i) wbase += wsum[i];
     uint64_t pos = offsets[seg] + wbase + incl - cnt;
-    const uint64_t lo = lo0 + (uint64_t)seg * span;
+    const uint64_t lo = seg_lo ? seg_lo[seg] : lo0 + (uint64_t)seg * span;
 #pragma unroll
     for (uint32_t i = 0; i < WPT; ++i) {
         uint32_t w = words[i];
@@ -184,16 +185,26 @@ __device__ bool is_prime64(uint64_t n) {
     return true;
 }
 
+// All ranges in one launch: range r owns blocks [d[r].block0, d[r].block0 +
+// ceil((hi - lo0) / 512)), one thread per odd number from its lo0, so only the
+// range's own integers are tested; its bitmap words and segment counts start
+// at d[r].word_off and d[r].seg_off (bitmap zeroed beforehand).
 __global__ void __launch_bounds__(256)
-k_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t* __restrict__ bitmap, uint32_t* __restrict__ seg_count) {
-    // one thread per odd number; a warp produces one bitmap word
-    const uint64_t bit = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t nval = lo0 + 2 * bit + 1;
-    const bool pr = (nval >= lo && nval < hi) ? is_prime64(nval) : false;
+k_window_primes_multi(const WinDesc* __restrict__ d, uint32_t nr, uint32_t* __restrict__ bitmap,
+                      uint32_t* __restrict__ seg_count) {
+    uint32_t a = 0, b = nr - 1;          // the last range with block0 <= blockIdx.x
+    while (a < b) {
+        const uint32_t m = (a + b + 1) >> 1;
+        if (d[m].block0 <= blockIdx.x) a = m; else b = m - 1;
+    }
+    const WinDesc w = d[a];
+    const uint64_t bit = (uint64_t)(blockIdx.x - w.block0) * blockDim.x + threadIdx.x;
+    const uint64_t nval = w.lo0 + 2 * bit + 1;
+    const bool pr = (nval >= w.lo && nval < w.hi) ? is_prime64(nval) : false;
     const uint32_t word = __ballot_sync(0xffffffffu, pr);
     if ((threadIdx.x & 31) == 0) {
-        bitmap[bit >> 5] = word;
-        if (word) atomicAdd(&seg_count[bit / SEG_BITS], (uint32_t)__popc(word));
+        bitmap[w.word_off + (bit >> 5)] = word;
+        if (word) atomicAdd(&seg_count[w.seg_off + bit / SEG_BITS], (uint32_t)__popc(word));
     }
 }
 
@@ -1713,13 +1724,17 @@ void launch_scan_counts(const uint32_t* counts, uint32_t n, uint64_t first, uint
 void launch_compact(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets,
                     uint32_t* out32, uint64_t* out64, cudaStream_t st) {
     if (!nseg) return;
-    k_compact<<<nseg, COMPACT_THREADS, 0, st>>>(lo0, SEG_SPAN, bitmap, offsets, out32, out64);
+    k_compact<<<nseg, COMPACT_THREADS, 0, st>>>(lo0, SEG_SPAN, bitmap, offsets, out32, out64, nullptr);
 }
-void launch_window_primes(uint64_t lo0, uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t* bitmap,
-                          uint32_t* seg_count, cudaStream_t st) {
+void launch_compact_multi(uint32_t nseg, const uint64_t* seg_lo, const uint32_t* bitmap, const uint64_t* offsets,
+                          uint64_t* out64, cudaStream_t st) {
     if (!nseg) return;
-    const uint64_t nbits = (uint64_t)nseg * SEG_BITS;
-    k_window_primes<<<(unsigned)(nbits / 256), 256, 0, st>>>(lo0, lo, hi, bitmap, seg_count);
+    k_compact<<<nseg, COMPACT_THREADS, 0, st>>>(0, SEG_SPAN, bitmap, offsets, nullptr, out64, seg_lo);
+}
+void launch_window_primes_multi(const WinDesc* d, uint32_t nr, uint32_t nblocks, uint32_t* bitmap,
+                                uint32_t* seg_count, cudaStream_t st) {
+    if (!nr || !nblocks) return;
+    k_window_primes_multi<<<nblocks, 256, 0, st>>>(d, nr, bitmap, seg_count);
 }
 void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys, uint64_t* out,
                       cudaStream_t st) {

@@ -135,7 +135,7 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
             std::vector<RangeState> rs;
             std::vector<uint64_t> tps;
             const int e = gen_test_primes(c, rr.data(), rr.size(), rs, tps, true);
-            s->ws.launches += 2 * rr.size();
+            s->ws.launches += 2;
             for (size_t j = 0; j < need.size(); ++j) {
                 SReq* q = cands[need[j]];
                 if (e) { result[need[j]] = e; continue; }

@@ -278,8 +278,10 @@ def run_serving(args, rank, world, local):
     reqs = serving_requests(1, args.requests, args.rate, args.max_width)[rank::world]
     L = max(limbs_for(b - 1) for _, a, b in reqs)
     peak_mad = wl.probe("mad", local)
+    # the default kernels unless asked: the tuner times the first requests as
+    # one batch, whose best choice can lengthen the serving latency tail
     tuning = None
-    if not args.no_autotune:
+    if args.serving_autotune:
         eng = wl.Engine(local)
         tuning = eng.autotune([(a, b) for _, a, b in reqs[:64]], q_cap)
         eng.close()
@@ -468,6 +470,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default kernel choices instead of timing the variants before the warm-up")
+    ap.add_argument("--serving-autotune", action="store_true",
+                    help="serving: tune the kernels on the first 64 requests run as one batch (batch throughput; "
+                         "the default kernels are kept otherwise)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -318,30 +318,31 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
 int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<RangeState>& rs,
                     std::vector<uint64_t>& tps, bool allow_empty) {
     rs.assign(nr, RangeState());
-    uint64_t words = 0, segs = 0;
+    std::vector<uint64_t> pmins(nr), pmaxs(nr);
+    for (size_t i = 0; i < nr; ++i) {
+        pmins[i] = ranges[i].pmin;
+        pmaxs[i] = ranges[i].pmax;
+    }
+    std::vector<WindowPlan> wp;
+    uint64_t words = 0, segs = 0, blocks = 0;
+    plan_windows(pmins.data(), pmaxs.data(), nr, SEG_SPAN, wp, &words, &segs, &blocks);
     for (size_t i = 0; i < nr; ++i) {
         RangeState& r = rs[i];
-        r.pmin = ranges[i].pmin;
-        r.pmax = ranges[i].pmax;
-        r.lo0 = r.pmin & ~1ull;
-        r.nseg = (uint32_t)((r.pmax - r.lo0 + SEG_SPAN - 1) / SEG_SPAN);
-        r.word_off = words;
-        r.seg_off = segs;
-        words += (uint64_t)r.nseg * SEG_WORDS;
-        segs += r.nseg;
+        r.pmin = pmins[i];
+        r.pmax = pmaxs[i];
+        r.lo0 = wp[i].lo0;
+        r.nseg = wp[i].nseg;
+        r.word_off = wp[i].word_off;
+        r.seg_off = wp[i].seg_off;
     }
     RC(ensure(c->bitmap, std::max<uint64_t>(words * 4, c->bitmap.cap)));
     RC(ensure(c->segcount, std::max<uint64_t>(segs * 4, c->segcount.cap)));
     RC(ensure(c->offsets, std::max<uint64_t>((segs + 1) * 8, c->offsets.cap)));
     // every range in one launch, each over its own integers only (512 per block)
-    std::vector<WinDesc> wd(nr);
-    uint64_t blocks = 0;
-    for (size_t i = 0; i < nr; ++i) {
-        const RangeState& r = rs[i];
-        wd[i] = WinDesc{ r.lo0, r.pmin, r.pmax, r.word_off, r.seg_off, (uint32_t)blocks, 0 };
-        blocks += (r.pmax - r.lo0 + 511) / 512;
-    }
     if (blocks >= (1ull << 31)) return WL_ERR_UNSUPPORTED;
+    std::vector<WinDesc> wd(nr);
+    for (size_t i = 0; i < nr; ++i)
+        wd[i] = WinDesc{ wp[i].lo0, pmins[i], pmaxs[i], wp[i].word_off, wp[i].seg_off, (uint32_t)wp[i].block0, 0 };
     RC(ensure(c->windesc, nr * sizeof(WinDesc)));
     CK(cudaMemcpyAsync(c->windesc.p, wd.data(), nr * sizeof(WinDesc), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemsetAsync(c->bitmap.p, 0, words * 4, c->st));

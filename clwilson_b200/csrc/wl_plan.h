@@ -1,6 +1,6 @@
 // wl_plan.h -- split planning of the column sweeps: how many splits each
-// bucket gets, and the cost model behind the dense sweep's split boundaries.
-// Host code only (no CUDA).
+// bucket gets, and the cost model behind the dense sweep's split boundaries;
+// the layout of the test-prime windows.  Host code only (no CUDA).
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -109,4 +109,37 @@ inline double split_scale(const std::vector<SplitBucket>& bs, double W, double t
         scale *= 0.9 * budget / tot;
     }
     return scale;
+}
+
+// Test-prime windows of a batch of ranges, for one launch over all of them.
+// Range i covers the odd numbers lo0 + 2j + 1 from lo0 = pmin rounded down to
+// even, in nseg segments of `seg_span` integers (seg_span / 64 bitmap words
+// and one prime counter each).  It owns ceil((pmax - lo0) / 512) blocks of
+// 256 threads, one thread per odd number, so only its own integers are
+// tested.  Its words, counters and blocks follow those of range i - 1.
+struct WindowPlan {
+    uint64_t lo0 = 0;
+    uint32_t nseg = 0;
+    uint64_t word_off = 0, seg_off = 0, block0 = 0, nblocks = 0;
+};
+
+inline void plan_windows(const uint64_t* pmin, const uint64_t* pmax, size_t nr, uint32_t seg_span,
+                         std::vector<WindowPlan>& out, uint64_t* words, uint64_t* segs, uint64_t* blocks) {
+    out.assign(nr, WindowPlan());
+    uint64_t w = 0, s = 0, b = 0;
+    for (size_t i = 0; i < nr; ++i) {
+        WindowPlan& p = out[i];
+        p.lo0 = pmin[i] & ~1ull;
+        p.nseg = (uint32_t)((pmax[i] - p.lo0 + seg_span - 1) / seg_span);
+        p.word_off = w;
+        p.seg_off = s;
+        p.block0 = b;
+        p.nblocks = (pmax[i] - p.lo0 + 511) / 512;
+        w += (uint64_t)p.nseg * (seg_span / 64);
+        s += p.nseg;
+        b += p.nblocks;
+    }
+    *words = w;
+    *segs = s;
+    *blocks = b;
 }

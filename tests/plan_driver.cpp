@@ -4,6 +4,9 @@
 //                      boundary k = 1 .. Sd-1 its q and the cumulative cost at q
 //   splits nrows rpt ndense nsparse dcost W threads scale     -> Sd Ss
 //   scale W threads budget (nrows ndense nsparse dcost)...    -> scale and partials
+//   windows seg_span (pmin pmax)...   test-prime window layout: totals (words
+//                      segs blocks), then per range lo0 nseg word_off seg_off
+//                      block0 nblocks
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -11,6 +14,22 @@
 #include "wl_plan.h"
 
 int main(int argc, char** argv) {
+    if (argc >= 3 && !strcmp(argv[1], "windows")) {
+        const uint32_t span = (uint32_t)strtoul(argv[2], nullptr, 0);
+        std::vector<uint64_t> lo, hi;
+        for (int i = 3; i + 1 < argc; i += 2) {
+            lo.push_back(strtoull(argv[i], nullptr, 0));
+            hi.push_back(strtoull(argv[i + 1], nullptr, 0));
+        }
+        std::vector<WindowPlan> wp;
+        uint64_t words = 0, segs = 0, blocks = 0;
+        plan_windows(lo.data(), hi.data(), lo.size(), span, wp, &words, &segs, &blocks);
+        printf("%" PRIu64 " %" PRIu64 " %" PRIu64 "\n", words, segs, blocks);
+        for (const WindowPlan& p : wp)
+            printf("%" PRIu64 " %u %" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 "\n", p.lo0, p.nseg, p.word_off,
+                   p.seg_off, p.block0, p.nblocks);
+        return 0;
+    }
     if (argc >= 5 && !strcmp(argv[1], "bounds")) {
         const double T = atof(argv[2]), qd = atof(argv[3]);
         const uint64_t Sd = strtoull(argv[4], nullptr, 0);

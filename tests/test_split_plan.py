@@ -9,7 +9,10 @@
   at 2,048 to 2^17 columns.
 * The memory budget lengthens splits so that the partials of the full
   top-of-range workload (2.3e5 rows, 2e8 dense columns) fit; without it the
-  1,024-column rule asks for about 740 GB."""
+  1,024-column rule asks for about 740 GB.
+* The test-prime window layout of a batch of ranges (one launch for all):
+  every odd number of each range has a thread of that range's blocks, and
+  the blocks stay within the range's own bitmap words and counters."""
 import os
 import subprocess
 
@@ -81,3 +84,53 @@ def test_memory_budget_top_of_range(driver):
     # unscaled, the 1,024-column rule alone would ask for ~740 GB of partials
     Sd, _ = _splits(driver, 78000, 2, 203_000_000, 0, 4.5 * 203_000_000, W, THREADS, 1.0)
     assert Sd * 78000 * 3 * 16 > 700e9
+
+
+def _windows(driver, ranges, span=1 << 18):
+    args = [driver, "windows", str(span)]
+    for lo, hi in ranges:
+        args += [str(lo), str(hi)]
+    lines = subprocess.run(args, capture_output=True, text=True, check=True).stdout.strip().splitlines()
+    words, segs, blocks = map(int, lines[0].split())
+    rows = [tuple(int(x) for x in ln.split()) for ln in lines[1:]]
+    return words, segs, blocks, rows
+
+
+def _random_ranges(seed, n):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    starts = np.exp(rng.uniform(np.log(5.0), np.log(2.0**62 - 2e7), n))
+    widths = np.exp(rng.uniform(0.0, np.log(1e7), n))
+    return [(int(s), int(s) + max(1, int(w))) for s, w in zip(starts, widths)]
+
+
+@pytest.mark.parametrize("ranges", [
+    [(10**9, 10**9 + 10**6)],
+    [(5, 6), (6, 7), (7, 8), (1 << 20, (1 << 20) + (1 << 18)), ((1 << 20) + 1, (1 << 20) + 1 + (1 << 18)),
+     ((1 << 62) - 10**7, (1 << 62) - 1), (10**6, 10**6 + 1)],
+    "random",
+])
+def test_window_layout(driver, ranges):
+    # the layout of k_window_primes_multi: every odd number of a range is one
+    # thread of that range's blocks, and its blocks write only that range's
+    # bitmap words and segment counters, which follow the previous range's
+    if ranges == "random":
+        ranges = _random_ranges(7, 300)
+    span = 1 << 18
+    words, segs, blocks, rows = _windows(driver, ranges, span)
+    assert len(rows) == len(ranges)
+    w = s = b = 0
+    for (lo, hi), (lo0, nseg, word_off, seg_off, block0, nblocks) in zip(ranges, rows):
+        assert lo0 == lo & ~1 and (word_off, seg_off, block0) == (w, s, b)
+        assert nseg * span >= hi - lo0 > (nseg - 1) * span
+        # odd numbers lo0 + 2j + 1 for j < nblocks * 256: all of [lo, hi), within the segments
+        first_j, last_j = (lo - lo0 - 1 + 1) // 2, (hi - 1 - lo0 - 1) // 2
+        assert 0 <= first_j and last_j < nblocks * 256
+        assert nblocks * 256 <= nseg * span // 2
+        # ceil((hi - lo0) / 512) blocks: the last starts at most one (even) integer past the range
+        assert nblocks == (hi - lo0 + 511) // 512
+        assert (nblocks - 1) * 256 <= last_j + 1
+        w += nseg * span // 64
+        s += nseg
+        b += nblocks
+    assert (words, segs, blocks) == (w, s, b)

@@ -368,6 +368,8 @@ def run_column_shard(args, rank, world, local):
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
     (lo, hi), = workload("column-shard", rank, world, args.width)[0]
     bounds = colshard.column_pieces(lo, hi, world)
+    if dist:
+        bounds = colshard.agree_on_bounds(bounds, rank)
     peak_mad = wl.probe("mad", local)
     L = limbs_for(hi - 1)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MiB > L2

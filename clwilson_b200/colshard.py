@@ -19,8 +19,11 @@ The rows, result lines and checksum are those of a one-GPU wl_search of the
 range.  The pieces partition the columns, and products mod p^2 do not depend
 on order.  The exchange is one gather of 16 bytes per row and rank.
 
-Multiply-rows and finish run only on rank 0.  With the NCCL backend every rank
-must have selected its CUDA device (torch.cuda.set_device) before the gather.
+The row-wise product and the finish run only on rank 0.  Every rank uses
+rank 0's piece boundaries (one broadcast), so the pieces partition the
+columns however each rank would have planned them.  With the NCCL backend
+every rank must have selected its CUDA device (torch.cuda.set_device) before
+the collectives.
 """
 from __future__ import annotations
 
@@ -209,6 +212,14 @@ def finish_pieces(engine, pmin: int, pmax: int, bounds: Sequence[int], parts: Se
     return engine.search_from(pmin, pmax, bounds[-1], init=init)
 
 
+def agree_on_bounds(bounds: List[int], rank: int, group=None) -> List[int]:
+    """Rank 0's piece boundaries on every rank (torch.distributed broadcast)."""
+    import torch.distributed as dist
+    box = [list(bounds) if rank == 0 else None]
+    dist.broadcast_object_list(box, src=0, group=group)
+    return box[0]
+
+
 def gather_to_rank0(obj, rank: int, world: int, group=None):
     """One object per rank, in rank order, on rank 0 (None elsewhere):
     torch.distributed.gather_object over `group`."""
@@ -225,8 +236,11 @@ def search_columns_sharded(engine, pmin: int, pmax: int, rank: int = 0, world: i
     Every rank calls this with its own engine (one GPU each).  Rank 0 returns
     the SearchResult; the other ranks return None.  `gather(obj)` collects
     one object per rank on rank 0 in rank order.  By default it is
-    torch.distributed.gather_object over `group`."""
+    torch.distributed.gather_object over `group`, and the boundaries are rank
+    0's, broadcast over `group`."""
     bounds = column_pieces(pmin, pmax, world)
+    if world > 1 and gather is None:
+        bounds = agree_on_bounds(bounds, rank, group)
     part = search_piece(engine, pmin, pmax, bounds, rank)
     if world == 1:
         return finish_pieces(engine, pmin, pmax, bounds, [part])

@@ -6,7 +6,8 @@ piece is charged the finish it also runs; the range model of narrow ranges
 has the oracle's class counts and targets.
 
 The flow: gloo ranks (world sizes 2 and 3) run search_columns_sharded with
-an engine whose calls are answered by the oracle.  The pieces are products
+an engine whose calls are answered by the oracle, also with the other ranks
+planning different boundaries (rank 0's are broadcast).  The pieces are products
 over disjoint column intervals (oracle.range_product).  The row-wise product
 uses exact integers, and the finishing call checks that its init is the
 oracle's product over all columns.  Rank 0 must return the oracle's full
@@ -140,12 +141,17 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, ranges, q):
+def _rank_main(rank, world, port, ranges, q, perturb=False):
     import datetime
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     import torch.distributed as dist
     from clwilson_b200 import colshard as cs
+    if perturb and rank > 0:
+        # this rank would plan other boundaries; rank 0's broadcast ones must win
+        plan = cs.column_pieces
+        cs.column_pieces = lambda lo, hi, w, **k: [b if i in (0, len(bs) - 1) else b + 1 + i
+                                                   for bs in [plan(lo, hi, w, **k)] for i, b in enumerate(bs)]
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
@@ -162,13 +168,13 @@ def _rank_main(rank, world, port, ranges, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_sharded_flow_matches_oracle(world):
+@pytest.mark.parametrize("world,perturb", [(2, False), (3, False), (3, True)])
+def test_sharded_flow_matches_oracle(world, perturb):
     ranges = [(200, 564), (10**6, 10**6 + 3000), (5, 8)]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    mp.start_processes(_rank_main, args=(world, _free_port(), ranges, q), nprocs=world, start_method="spawn",
-                       join=True)
+    mp.start_processes(_rank_main, args=(world, _free_port(), ranges, q, perturb), nprocs=world,
+                       start_method="spawn", join=True)
     got = q.get(timeout=60)
     for (pmin, pmax), (lines, ck, fin) in zip(ranges, got):
         full, _ = oracle.search(pmin, pmax)

@@ -27,6 +27,22 @@ def test_library_loads_and_exports_header_symbols():
     assert set(wl.SYMBOLS) >= set(syms)
 
 
+def test_bindings_match_header_arity():
+    # every declared function has a ctypes binding with as many parameters as
+    # its declaration (a mismatch passes garbage across the C ABI)
+    import glob
+    src = "".join(open(h).read() for h in glob.glob(os.path.join(ROOT, "include", "*.h")))
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    decls = re.findall(r"\b(?:int|void|const char\s*\*|void\s*\*)\s*\*?\s*(wl_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src)
+    assert len(decls) >= len(declared_symbols())
+    L = wl.load_library()
+    for name, params in decls:
+        p = params.strip()
+        n = 0 if p in ("", "void") else p.count(",") + 1
+        argtypes = getattr(L, name).argtypes
+        assert argtypes is not None and len(argtypes) == n, (name, n, argtypes)
+
+
 def test_strerror():
     L = wl.load_library()
     assert L.wl_strerror(-3) == b"there are no primes to test in this range!"

@@ -31,6 +31,15 @@ sweep, tail, lift, results).  `value` is device time (CUDA events on the
 engine's stream, L2 flushed between steps); `e2e` is host wall time around the
 same C-ABI call, which includes its host<->device copies.
 
+The default run (plain-small) adds two records to its line, so that one run
+measures the whole metric: `batched` (the 256 ranges, widths truncated to
+--sub-batched-width, one warm-up call and --sub-batched-steps timed calls,
+then the plain per-range form over the same ranges) and `serving` (the first
+--sub-serving-requests requests of the default_rng(1) stream at
+--sub-serving-rate per second, widths truncated to 2,000).  Every line also
+carries `parity_sample`: the engine's rows at the CPU baseline's sample
+indices, compared with the oracle's bit for bit.
+
 --impl reference times the reference algorithm on the host cores instead (the
 CPU restatement under oracle/, all threads) on a bounded sample of the same
 workload.
@@ -51,6 +60,38 @@ sys.path.insert(0, ROOT)
 
 PLAIN_SMALL = (10**9, 10**6)
 OPS_PER_CELL = {2: 9, 3: 13, 4: 17}   # multiply-class PTX ops of one cell step (wl_arith.cuh)
+HBM_FALLBACK_GBS = 6650.0             # copy bandwidth measured earlier on this kind of GPU
+
+
+def hbm_peak():
+    """(GB/s, source) of the HBM roofline: the measured copy bandwidth when a
+    peaks file is present, else the earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "of measured"
+    except Exception:
+        pass
+    return HBM_FALLBACK_GBS, "of fallback"
+
+
+def work_cells(st, L):
+    """Cells the sweeps executed in cell-equivalents: one per (row, column)
+    of every column, the dense sweep's window cells, and its full products
+    (about L cells each); and the dense share of them."""
+    extra = st.dense_window_cells + L * st.dense_products
+    return st.cells + extra, st.dense_column_cells + extra
+
+
+def parity_sample(eng, lo, hi, q_cap, want, sel):
+    """The engine's rows of [lo, hi) at rows `sel` against the oracle's
+    (`want`, the rows the CPU baseline computed): every field bit for bit."""
+    got, _ = eng.rows(lo, hi, q_cap=q_cap)
+    fields = ("p", "s0", "s1") + (() if q_cap else ("rem", "quot", "status"))
+    ok = len(got) == len(want) and all(int(got[f][i]) == int(want[f][i]) for i in sel for f in fields)
+    return {"ok": bool(ok), "rows_compared": len(sel), "range": [lo, hi], "fields": list(fields)}
 
 
 def limbs_for(pmax_incl: int) -> int:
@@ -201,14 +242,23 @@ def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
         step = max(1, n // k)
         sel = list(range(0, n, step))[:k]
         t0 = time.perf_counter()
-        rows, _ = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        rows, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
         dt = time.perf_counter() - t0
-        if dt > budget_s / 3 or k >= n or k >= 64 * cores:
+        if dt > budget_s / 3 or k >= n or k >= 512 * cores:
             break
         k *= 2
+    # the oracle sieves its columns on one thread in every call; time that part alone
+    limit = max(int(t) for t in targets) + 1
+    if q_cap:
+        limit = min(limit, q_cap)
+    t0 = time.perf_counter()
+    oracle.count_primes_below(limit)
+    sieve_s = time.perf_counter() - t0
     return {"value": len(sel) / dt, "unit": "primes/s", "cores": cores, "kind": "port",
             "sample": f"{len(sel)} of {n} primes of [{lo}, {hi}) evenly spaced, q_cap={q_cap}, "
-                      f"{dt:.1f} s incl. the column sieve"}, rows, sel
+                      f"{dt:.1f} s incl. the column sieve",
+            "sieve_share": sieve_s / dt,
+            "value_without_sieve": len(sel) / max(dt - sieve_s, 1e-9)}, rows, sel
 
 
 def run_reference(args, rank, world):
@@ -227,8 +277,8 @@ def run_reference(args, rank, world):
     while True:
         sel = list(range(0, n, max(1, n // k)))[:k]
         t0 = time.perf_counter()
-        oracle.search(lo, hi, qcap=q_cap, rows=sel)
-        if time.perf_counter() - t0 > 5.0 or k >= n or k >= 64 * cores:
+        _, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        if time.perf_counter() - t0 > 5.0 or k >= n or k >= 512 * cores:
             break
         k *= 2
     times = []
@@ -239,6 +289,13 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
+    # the share of a step the oracle spends sieving its columns (one thread)
+    limit = max(int(t) for t in targets) + 1
+    if q_cap:
+        limit = min(limit, q_cap)
+    t0 = time.perf_counter()
+    oracle.count_primes_below(limit)
+    sieve_s = time.perf_counter() - t0
     if q_cap:
         # the capped sweep's unit: column cells (sieving primes q <= T, q < q_cap) of the sampled rows
         per_class = [oracle.count_primes_below(min(t, q_cap - 1) + 1) if t else 0 for t in targets]
@@ -254,40 +311,25 @@ def run_reference(args, rank, world):
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": desc, "sample_rows_per_step": len(sel), "rows_in_workload": n},
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
-                         "sample": f"{len(sel)} of {n} primes per step, evenly spaced, q_cap={q_cap}"},
+                         "sample": f"{len(sel)} of {n} primes per step, evenly spaced, q_cap={q_cap}",
+                         "sieve_share": sieve_s / (tot / len(times))},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_serving(args, rank, world, local):
-    """The serving stream: submit each request at its arrival time, wait for
-    all, report throughput over the stream and request latencies."""
+def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, warmup, tuning=None):
+    """The serving stream through a serving session: every request submitted
+    at its arrival time, all waited for.  Returns the record (throughput over
+    the device-busy time, e2e over the stream's wall time, latencies)."""
     import numpy as np
-    import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
     import clwilson_b200 as wl
-    q_cap = 2**28 if args.qcap < 0 else args.qcap
-    reqs = serving_requests(1, args.requests, args.rate, args.max_width)[rank::world]
+    reqs = serving_requests(1, requests, rate, max_width)[rank::world]
     L = max(limbs_for(b - 1) for _, a, b in reqs)
-    peak_mad = wl.probe("mad", local)
-    # the default kernels unless asked: the tuner times the first requests as
-    # one batch, whose best choice can lengthen the serving latency tail
-    tuning = None
-    if args.serving_autotune:
-        eng = wl.Engine(local)
-        tuning = eng.autotune([(a, b) for _, a, b in reqs[:64]], q_cap)
-        eng.close()
     srv = wl.Server(local, tuning=tuning)
 
-    def stream(reqs, clk=None):
+    def stream(reqs):
         ids = []
         t0 = time.perf_counter()
         for t, a, b in reqs:
@@ -302,7 +344,7 @@ def run_serving(args, rank, world, local):
         return infos, t1 - t0
 
     # warm-up: a few requests through the session (column cache, first launches)
-    for _ in range(max(3, args.warmup)):
+    for _ in range(warmup):
         stream(reqs[:4])
     st0 = srv.stats()
     if dist:
@@ -310,44 +352,163 @@ def run_serving(args, rank, world, local):
     with ClockSampler(local) as clk:
         infos, wall = stream(reqs)
     st1 = srv.stats()
+    srv.close()
+    d = {k: st1[k] - st0[k] for k in ("steps", "admitted", "completed", "launches", "ms_steps", "ms_admit",
+                                      "ms_wall_steps", "ms_wall_admit", "ms_wall_finish")}
     bad = [i for i in infos if i.state != "done"]
     cells = sum(i.cells for i in infos)
     rows = sum(i.tested for i in infos)
-    busy_s = ((st1["ms_steps"] - st0["ms_steps"]) + (st1["ms_admit"] - st0["ms_admit"])) / 1e3
-    lat = np.array([i.ms_latency for i in infos])
-    (wall, busy_s), (cells, rows) = merge_over_ranks(dist, [wall, busy_s], [cells, rows])
-    line = {
+    busy_s = (d["ms_steps"] + d["ms_admit"]) / 1e3
+    lat = [i.ms_latency for i in infos]
+    queued = [i.ms_queued for i in infos]
+    if dist:
+        every = [None] * world
+        dist.all_gather_object(every, (lat, queued))
+        lat = [x for l, _ in every for x in l]
+        queued = [x for _, qd in every for x in qd]
+    lat = np.array(lat)
+    (wall, busy_s), (cells, rows, nreq, nbad) = merge_over_ranks(dist, [wall, busy_s],
+                                                                 [cells, rows, len(reqs), len(bad)])
+    host_us = 1e3 * (d["ms_wall_steps"] - d["ms_steps"]) / max(1, d["steps"])
+    return {
         "metric": "128-bit mulmods/s (capped column sweep, serving)", "value": cells / busy_s,
-        "unit": "mulmods/s", "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup),
-        "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"serving: {len(reqs)} requests from default_rng(1), Poisson at {args.rate}/s, "
-                               f"widths truncated to {args.max_width}, columns q < {q_cap}",
-                   "rate_per_s": args.rate, "requests": len(reqs), "q_cap": q_cap, "limbs_max": L,
+        "unit": "mulmods/s", "higher_is_better": True, "n_gpus": world, "steps": 1, "warmup": warmup,
+        "ms_per_step": 1e3 * wall,
+        "config": {"workload": f"serving: {int(nreq)} requests from default_rng(1), Poisson at {rate}/s, "
+                               f"widths truncated to {max_width}, columns q < {q_cap}",
+                   "rate_per_s": rate, "requests": int(nreq), "q_cap": q_cap, "limbs_max": L,
                    "test_primes": rows, "column_mulmods": cells,
-                   "l2": "inputs (row pool + column table) exceed L2 across the stream",
                    "parallelism": f"requests sharded round-robin, dp{world}"},
         "e2e": {"value": cells / wall, "unit": "mulmods/s", "primes_per_s": rows / wall,
-                "h2d_bytes_per_step": 16 * len(reqs), "d2h_bytes_per_step": 48 * int(rows)},
+                "h2d_bytes_per_step": 16 * int(nreq), "d2h_bytes_per_step": 48 * int(rows)},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "max": float(lat.max()), "mean": float(lat.mean())},
-        "queue_ms_p50": float(np.percentile([i.ms_queued for i in infos], 50)),
-        "failed": len(bad),
-        "server": {k: st1[k] - st0[k] for k in ("steps", "admitted", "completed", "launches")} |
-                  {"peak_active": st1["peak_active"], "busy_s": busy_s},
-        "gpu_launches": st1["launches"] - st0["launches"],
-        "tuning": tuning if tuning is not None else "defaults",
-        "roofline": {"bound": "imad", "peak": peak_mad / 1e12, "unit": "TOP/s", "achieved": None, "frac": None,
-                     "traffic": None, "note": "device-busy throughput; see the batched and plain lines for the kernels",
-                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
+                       "max": float(lat.max()), "mean": float(lat.mean()), "requests": int(lat.size)},
+        "queue_ms_p50": float(np.percentile(queued, 50)),
+        "failed": int(nbad),
+        "server": {"steps": d["steps"], "admitted": d["admitted"], "completed": d["completed"],
+                   "launches": d["launches"], "peak_active": st1["peak_active"], "busy_s": busy_s,
+                   "host_us_per_step": host_us,
+                   "device_us_per_step": 1e3 * d["ms_steps"] / max(1, d["steps"]),
+                   "wall_s": {"steps": d["ms_wall_steps"] / 1e3, "admit": d["ms_wall_admit"] / 1e3,
+                              "finish": d["ms_wall_finish"] / 1e3}},
+        "gpu_launches": d["launches"],
         "clocks": clk.summary(),
     }
+
+
+def run_serving(args, rank, world, local):
+    """The serving stream as its own line."""
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import clwilson_b200 as wl
+    q_cap = 2**28 if args.qcap < 0 else args.qcap
+    peak_mad = wl.probe("mad", local)
+    # the default kernels unless asked: the tuner times the first requests as
+    # one batch, whose best choice can lengthen the serving latency tail
+    tuning = None
+    if args.serving_autotune:
+        reqs = serving_requests(1, args.requests, args.rate, args.max_width)[rank::world]
+        eng = wl.Engine(local)
+        tuning = eng.autotune([(a, b) for _, a, b in reqs[:64]], q_cap)
+        eng.close()
+    line = serving_record(local, rank, world, dist, args.requests, args.rate, args.max_width, q_cap,
+                          max(3, args.warmup), tuning)
+    line.update({"scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                 "tuning": tuning if tuning is not None else "defaults",
+                 "roofline": {"bound": "imad", "peak": peak_mad / 1e12, "unit": "TOP/s", "achieved": None,
+                              "frac": None, "traffic": None,
+                              "note": "device-busy throughput; see the batched and plain lines for the kernels",
+                              "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"}})
     if rank == 0:
         print(json.dumps(line), flush=True)
-    srv.close()
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def batched_record(eng, rank, world, dist, stream, flush, max_width, steps, plain_steps):
+    """The batched workload (256 ranges from default_rng(0), widths truncated
+    to max_width, q < 2^28) through wl_batch, one warm-up call, `steps` timed
+    calls, and the same ranges as a loop of per-range calls (the plain form)."""
+    import torch
+    ranges, q_cap, desc = workload("batched", rank, world, max_width=max_width)
+    per_range_rows = []
+
+    def timed(fn):
+        flush.add_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        out = fn()
+        t1 = time.perf_counter()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3, t1 - t0
+
+    def batch():
+        eng.drop_columns()
+        return eng.batch(ranges, q_cap=q_cap)
+
+    def plain():
+        eng.drop_columns()
+        cks, cells = [], 0
+        for a, b in ranges:
+            rows, st = eng.rows(a, b, q_cap=q_cap)
+            cks.append(int((rows["p"].astype(object) + rows["s0"].astype(object)
+                            + rows["s1"].astype(object)).sum()) % (1 << 64))
+            cells += st.cells
+        return cks, cells
+
+    per_b, _, _ = batch()                          # warm-up
+    per_range_rows = [pb["tested"] for pb in per_b]
+    if dist:
+        dist.barrier()
+    dev, wall, stats = [], [], []
+    for _ in range(steps):
+        (_, _, st), d, w = timed(batch)
+        dev.append(d)
+        wall.append(w)
+        stats.append(st)
+    pdev, pwall, cks = [], [], None
+    for _ in range(plain_steps):
+        (cks, cells_p), d, w = timed(plain)
+        pdev.append(d)
+        pwall.append(w)
+    cells = sum(s.cells for s in stats)
+    rows = sum(s.tested for s in stats)
+    sweep_s = sum(s.ms_sweep for s in stats) / 1e3
+    work = [work_cells(s, 4) for s in stats]
+    (tot_dev, tot_wall, sweep_s, pd, pw), (cells_all, rows_all, work_all, dense_all, pcells) = merge_over_ranks(
+        dist, [sum(dev), sum(wall), sweep_s, sum(pdev), sum(pwall)],
+        [cells, rows, sum(w for w, _ in work), sum(x for _, x in work), cells_p * len(pdev) if pdev else 0])
+    rec = {
+        "metric": "128-bit mulmods/s (capped column sweep, batched)", "value": cells_all / tot_dev,
+        "unit": "mulmods/s", "steps": steps, "warmup": 1, "ms_per_step": 1e3 * tot_dev / steps,
+        "config": {"workload": desc, "q_cap": q_cap, "ranges": len(ranges),
+                   "test_primes_per_step": rows_all / steps, "column_mulmods_per_step": cells_all / steps,
+                   "rows_per_range": {"min": int(min(per_range_rows)), "max": int(max(per_range_rows))},
+                   "l2": "256 MiB buffer written between steps", "columns": "re-sieved every step"},
+        "e2e": {"value": cells_all / tot_wall, "unit": "mulmods/s"},
+        "gpu_launches": sum(s.kernel_launches for s in stats),
+        "work": {"cell_equivalents_per_step": work_all / steps, "dense_share": dense_all / max(1.0, work_all),
+                 "cell_equivalents_per_s_in_sweep": work_all / max(sweep_s, 1e-9),
+                 "note": "every column cell, plus the dense sweep's window cells and its full products at "
+                         "L = 4 cells each"},
+    }
+    if pdev:
+        rec["plain_form"] = {"value": pcells / pd, "unit": "mulmods/s", "e2e": pcells / pw,
+                             "ms_per_pass": 1e3 * pd / len(pdev), "passes": len(pdev),
+                             "calls_per_pass": len(ranges),
+                             "per_range_checksums_equal": [pb["checksum"] for pb in per_b] == cks}
+        rec["batched_over_plain"] = rec["value"] / rec["plain_form"]["value"]
+    return rec
 
 
 def run_column_shard(args, rank, world, local):
@@ -379,7 +540,14 @@ def run_column_shard(args, rank, world, local):
         part, st = None, None
         if rank < len(bounds) - 1:
             part, st = eng.rows_from(lo, hi, bounds[rank], bounds[rank + 1])
-        parts = [part] if world == 1 else colshard.gather_to_rank0(colshard.piece_digits(part), rank, world)
+        else:
+            part, _ = eng.rows_from(lo, hi, 2, 2)       # no piece: the empty product
+        if world == 1:
+            parts = [part]
+        else:
+            mine = colshard.piece_digits(part, colshard.piece_interval(bounds, rank))
+            parts = colshard.gather_to_rank0(mine, rank, world)
+            parts = colshard.check_pieces(bounds, parts) if rank == 0 else None
         res = colshard.finish_pieces(eng, lo, hi, bounds, parts, p=part["p"]) if rank == 0 else None
         return st, res
 
@@ -443,8 +611,12 @@ def run_column_shard(args, rank, world, local):
     if rank == 0:
         one = eng.search(lo, hi)
         line["checksum_equal_one_call"] = all(r.checksum == one.checksum and r.results == one.results for r in fins)
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"], _, _ = cpu_baseline(lo, hi, 0)
+        if not args.no_cpu_baseline:
+            cb, want, sel = cpu_baseline(lo, hi, 0, 20.0 if world == 1 else 5.0)
+            if world == 1:
+                line["cpu_baseline"] = cb
+            line["parity_sample"] = parity_sample(eng, lo, hi, 0, want, sel)
+            line["parity_sample_ok"] = line["parity_sample"]["ok"]
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:
@@ -475,6 +647,13 @@ def main():
     ap.add_argument("--serving-autotune", action="store_true",
                     help="serving: tune the kernels on the first 64 requests run as one batch (batch throughput; "
                          "the default kernels are kept otherwise)")
+    ap.add_argument("--no-sub-records", action="store_true",
+                    help="plain-small: skip the batched and serving records that the default run adds")
+    ap.add_argument("--sub-batched-width", type=int, default=20000,
+                    help="batched record: truncate each of the 256 ranges to this many integers")
+    ap.add_argument("--sub-batched-steps", type=int, default=1, help="batched record: timed calls")
+    ap.add_argument("--sub-serving-requests", type=int, default=2000, help="serving record: requests in the stream")
+    ap.add_argument("--sub-serving-rate", type=float, default=64.0, help="serving record: arrivals per second")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -558,7 +737,11 @@ def main():
         dist, [tot_dev, tot_wall, sweep_s], [tested, cells, launches])
 
     full = q_cap == 0
-    achieved = cells * OPS_PER_CELL[L] / sweep_s / 1e12
+    # cells the sweep kernels executed: every column cell, and in the dense
+    # regime the window cells and full products counted on the device
+    exec_cells = sum(work_cells(s, L)[0] for s in stats)
+    dense_cells = sum(work_cells(s, L)[1] for s in stats)
+    achieved = exec_cells * OPS_PER_CELL[L] / sweep_s / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -582,9 +765,14 @@ def main():
         "mulmods_per_s": cells_all / tot_dev,
         "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_mad / 1e12, "unit": "TOP/s",
                      "frac": achieved * 1e12 / peak_mad, "traffic": traffic,
-                     "kernel": f"k_sweep<{L},*>", "ops_per_cell": OPS_PER_CELL[L],
-                     "cell_peak_per_s": peak_cell, "cell_frac": (cells / sweep_s) / peak_cell,
-                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run"},
+                     "kernel": f"k_sweep<{L},*>" if dense_cells < 0.5 * exec_cells else f"k_sweep_dense<{L},*>",
+                     "ops_per_cell": OPS_PER_CELL[L],
+                     "cells_executed_per_step": exec_cells / args.steps,
+                     "dense_share_of_cells": dense_cells / max(1.0, exec_cells),
+                     "cell_peak_per_s": peak_cell, "cell_frac": (exec_cells / sweep_s) / peak_cell,
+                     "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run",
+                     "count": "cells executed: one per (row, column), plus the dense sweep's window cells and "
+                              "its full products at L cells each (device counters)"},
         "e2e": {"value": (tested_all / tot_wall) if full else (cells_all / tot_wall),
                 "unit": "primes/s" if full else "mulmods/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -595,6 +783,18 @@ def main():
         "phase_ms_per_step": {k: sum(getattr(s, "ms_" + k) for s in stats) / args.steps
                               for k in ("primes", "sieve", "sweep", "iterate", "finish")},
     }
+    # the column sieve (q < 2^32): its device-memory traffic over its event time
+    sieve_ms = sum(s.ms_sieve for s in stats)
+    if sieve_ms > 0:
+        peak_gbs, src = hbm_peak()
+        gbs = sum(s.sieve_bytes for s in stats) / (sieve_ms / 1e3) / 1e9
+        line["sieve"] = {"ms_per_step": sieve_ms / args.steps,
+                         "integers_per_step": sum(s.sieve_integers for s in stats) / args.steps,
+                         "bytes_per_step": sum(s.sieve_bytes for s in stats) / args.steps,
+                         "gbs": gbs, "hbm_peak_gbs": peak_gbs, "hbm_frac": gbs / peak_gbs, "peak_source": src,
+                         "integers_per_s": sum(s.sieve_integers for s in stats) / (sieve_ms / 1e3),
+                         "bound": "shared-memory marking (the bitmap is built in shared memory; HBM carries "
+                                  "the bitmap, counts and the ordered column table)"}
     if len(ranges) > 1 and args.plain_steps > 0:
         # the plain form: one wl_search per range, same ranges, same column cap
         per_b, _, _ = eng.batch(ranges, q_cap=q_cap)
@@ -634,12 +834,23 @@ def main():
             "per_range_checksums_equal": [pb["checksum"] for pb in per_b] == cks,
         }
         line["batched_over_plain"] = line["value"] / line["plain_form"]["value"]
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline:
+        # the oracle on a sample of rows: the CPU baseline (one GPU), and in
+        # every run the check of the engine's rows at the same indices
         lo, hi = max(ranges, key=lambda r: r[1] - r[0])
-        cb, _, _ = cpu_baseline(lo, hi, q_cap)
+        cb, want, sel = cpu_baseline(lo, hi, q_cap, 20.0 if world == 1 else 5.0)
         if not full:
             cb["note"] = "capped sweep: value is primes/s of the capped partial products"
-        line["cpu_baseline"] = cb
+        if world == 1:
+            line["cpu_baseline"] = cb
+        line["parity_sample"] = parity_sample(eng, lo, hi, q_cap, want, sel)
+        line["parity_sample_ok"] = line["parity_sample"]["ok"]
+    if args.workload == "plain-small" and not args.no_sub_records:
+        # the rest of the headline metric: batched against plain, and serving latency
+        line["batched"] = batched_record(eng, rank, world, dist, stream, flush, args.sub_batched_width,
+                                         args.sub_batched_steps, 1)
+        line["serving"] = serving_record(local, rank, world, dist, args.sub_serving_requests,
+                                         args.sub_serving_rate, 2000, 2**28, 3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

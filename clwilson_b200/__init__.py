@@ -67,7 +67,10 @@ class _Stats(ctypes.Structure):
                 ("checksum", ctypes.c_uint64), ("results", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
                 ("ms_device", ctypes.c_double), ("ms_primes", ctypes.c_double), ("ms_sieve", ctypes.c_double),
                 ("ms_sweep", ctypes.c_double), ("ms_iterate", ctypes.c_double), ("ms_finish", ctypes.c_double),
-                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double)]
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double),
+                ("sieve_integers", ctypes.c_uint64), ("sieve_bytes", ctypes.c_uint64),
+                ("dense_column_cells", ctypes.c_uint64), ("dense_window_cells", ctypes.c_uint64),
+                ("dense_products", ctypes.c_uint64)]
 
 
 class _Tuning(ctypes.Structure):
@@ -108,7 +111,9 @@ class _ServerStats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_uint64), ("admitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("cancelled", ctypes.c_uint64), ("rows_done", ctypes.c_uint64),
                 ("cells", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("ms_steps", ctypes.c_double),
-                ("ms_admit", ctypes.c_double), ("peak_rows", ctypes.c_uint32), ("peak_active", ctypes.c_uint32)]
+                ("ms_admit", ctypes.c_double), ("peak_rows", ctypes.c_uint32), ("peak_active", ctypes.c_uint32),
+                ("ms_wall_steps", ctypes.c_double), ("ms_wall_admit", ctypes.c_double),
+                ("ms_wall_finish", ctypes.c_double)]
 
 
 REQ_STATES = {0: "queued", 1: "active", 2: "done", 3: "cancelled", 4: "failed"}
@@ -125,8 +130,7 @@ SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", 
            "wl_column_product_noalloc", "wl_get_tuning", "wl_set_tuning", "wl_autotune",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
-PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5, "dfma": 6, "mad+dfma": 7,
-          "madwide+dfma": 8, "cell2fp64": 9, "cell2mix": 10}
+PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5}
 
 _lib = None
 
@@ -236,12 +240,18 @@ class Stats:
     h2d_bytes: int = 0
     d2h_bytes: int = 0
     ms_big: float = 0.0
+    sieve_integers: int = 0
+    sieve_bytes: int = 0
+    dense_column_cells: int = 0
+    dense_window_cells: int = 0
+    dense_products: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.tested, tuple(s.per_class), tuple(s.targets), s.pi_maxtarget, s.cells, s.tail_steps,
                    s.checksum, s.results, s.kernel_launches, s.ms_device, s.ms_primes, s.ms_sieve, s.ms_sweep,
-                   s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes, s.ms_big)
+                   s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes, s.ms_big, s.sieve_integers, s.sieve_bytes,
+                   s.dense_column_cells, s.dense_window_cells, s.dense_products)
 
 
 @dataclass

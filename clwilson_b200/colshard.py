@@ -17,13 +17,19 @@ and column sieve; rank 0 is charged the finish it also runs).
 
 The rows, result lines and checksum are those of a one-GPU wl_search of the
 range.  The pieces partition the columns, and products mod p^2 do not depend
-on order.  The exchange is one gather of 16 bytes per row and rank.
+on order.  The exchange is one tensor gather of 16 bytes per row and rank,
+after a 16-byte header that names the piece's column interval.
 
 The row-wise product and the finish run only on rank 0.  Every rank uses
 rank 0's piece boundaries (one broadcast), so the pieces partition the
-columns however each rank would have planned them.  With the NCCL backend
-every rank must have selected its CUDA device (torch.cuda.set_device) before
-the collectives.
+columns however each rank would have planned them; rank 0 also checks every
+gathered header against its boundaries and raises on a mismatch, which
+covers a caller-supplied gather too.  With the NCCL backend every rank must
+have selected its CUDA device (torch.cuda.set_device) before the collectives.
+
+The consecutive-integer tail stays in rank 0's finish.  The planner charges
+rank 0 for it (a smaller first piece), so the ranks' work is balanced with
+the tail where it is.
 """
 from __future__ import annotations
 
@@ -184,21 +190,51 @@ def column_pieces(pmin: int, pmax: int, world: int, rank0_extra: Optional[float]
 
 
 def search_piece(engine, pmin: int, pmax: int, bounds: Sequence[int], rank: int):
-    """Rank `rank`'s partial products (rows), or None when it holds no piece."""
+    """Rank `rank`'s partial products (rows).  A rank beyond the last piece
+    (a range with fewer columns than ranks) holds the empty product: every
+    row's digits (1, 0), from a call with no column (q_cap = 2)."""
     if rank >= len(bounds) - 1:
-        return None
+        rows, _ = engine.rows_from(pmin, pmax, 2, 2)
+        return rows
     rows, _ = engine.rows_from(pmin, pmax, bounds[rank], bounds[rank + 1])
     return rows
 
 
-def piece_digits(rows):
-    """The digits (s0, s1) of a piece's rows as an (n, 2) uint64 array: the
-    16 bytes per row that cross to rank 0."""
+def piece_interval(bounds: Sequence[int], rank: int):
+    """The column interval [lo, hi) of rank `rank`'s piece; (0, 0) for none."""
+    return (bounds[rank], bounds[rank + 1]) if rank < len(bounds) - 1 else (0, 0)
+
+
+def piece_digits(rows, interval=None):
+    """What crosses to rank 0 for one piece, as an (n + 1, 2) uint64 array:
+    the piece's column interval [lo, hi) in the first row, then the digits
+    (s0, s1) of every row, 16 bytes each.  Without `interval`, the (n, 2)
+    digits alone."""
     if rows is None:
         return None
-    out = np.empty((rows.size, 2), dtype=np.uint64)
-    out[:, 0] = rows["s0"]
-    out[:, 1] = rows["s1"]
+    head = 0 if interval is None else 1
+    out = np.empty((rows.size + head, 2), dtype=np.uint64)
+    if head:
+        out[0] = interval
+    out[head:, 0] = rows["s0"]
+    out[head:, 1] = rows["s1"]
+    return out
+
+
+def check_pieces(bounds: Sequence[int], parts: Sequence) -> List:
+    """The digit arrays of gathered pieces after checking each header against
+    rank 0's boundaries: piece r must cover [bounds[r], bounds[r + 1]), ranks
+    beyond the last piece hold (0, 0).  Raises ValueError on a mismatch (pieces
+    that overlap or leave a gap would give wrong quotients with no error)."""
+    out = []
+    for r, x in enumerate(parts):
+        want = piece_interval(bounds, r)
+        got = (int(x[0, 0]), int(x[0, 1]))
+        if got != tuple(want):
+            raise ValueError("column pieces disagree: rank %d swept [%d, %d), rank 0 planned [%d, %d)"
+                             % (r, got[0], got[1], want[0], want[1]))
+        if r < len(bounds) - 1:
+            out.append(x[1:])
     return out
 
 
@@ -220,13 +256,21 @@ def agree_on_bounds(bounds: List[int], rank: int, group=None) -> List[int]:
     return box[0]
 
 
-def gather_to_rank0(obj, rank: int, world: int, group=None):
-    """One object per rank, in rank order, on rank 0 (None elsewhere):
-    torch.distributed.gather_object over `group`."""
+def gather_to_rank0(arr, rank: int, world: int, group=None):
+    """Every rank's (n + 1, 2) uint64 array, in rank order, on rank 0 (None
+    elsewhere): one torch.distributed.gather of a tensor of 16 (n + 1) bytes
+    per rank, on the GPU for the NCCL backend and on the CPU otherwise.  All
+    ranks hold the same rows, so the shapes agree."""
+    import torch
     import torch.distributed as dist
-    out = [None] * world if rank == 0 else None
-    dist.gather_object(obj, out, dst=0, group=group)
-    return out
+    on_gpu = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    t = torch.from_numpy(np.ascontiguousarray(arr).view(np.int64)).to(dev)
+    bufs = [torch.empty_like(t) for _ in range(world)] if rank == 0 else None
+    dist.gather(t, bufs, dst=0, group=group)
+    if rank != 0:
+        return None
+    return [b.cpu().numpy().view(np.uint64) for b in bufs]
 
 
 def search_columns_sharded(engine, pmin: int, pmax: int, rank: int = 0, world: int = 1, group=None,
@@ -234,19 +278,20 @@ def search_columns_sharded(engine, pmin: int, pmax: int, rank: int = 0, world: i
     """One range searched with its columns split over `world` ranks.
 
     Every rank calls this with its own engine (one GPU each).  Rank 0 returns
-    the SearchResult; the other ranks return None.  `gather(obj)` collects
-    one object per rank on rank 0 in rank order.  By default it is
-    torch.distributed.gather_object over `group`, and the boundaries are rank
-    0's, broadcast over `group`."""
+    the SearchResult; the other ranks return None.  `gather(arr)` collects
+    one array per rank on rank 0 in rank order.  By default it is a tensor
+    gather over `group` (gather_to_rank0), and the boundaries are rank 0's,
+    broadcast over `group`.  With a caller's gather each rank plans its own
+    boundaries; rank 0 raises if any rank's piece differs from its plan."""
     bounds = column_pieces(pmin, pmax, world)
     if world > 1 and gather is None:
         bounds = agree_on_bounds(bounds, rank, group)
     part = search_piece(engine, pmin, pmax, bounds, rank)
     if world == 1:
         return finish_pieces(engine, pmin, pmax, bounds, [part])
-    mine = piece_digits(part)
+    mine = piece_digits(part, piece_interval(bounds, rank))
     parts = gather(mine) if gather is not None else gather_to_rank0(mine, rank, world, group)
     if rank != 0:
         return None
     # rank 0 always holds the first piece, whose rows carry the primes
-    return finish_pieces(engine, pmin, pmax, bounds, parts, p=part["p"])
+    return finish_pieces(engine, pmin, pmax, bounds, check_pieces(bounds, parts), p=part["p"])

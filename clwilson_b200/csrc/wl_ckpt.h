@@ -2,7 +2,24 @@
 // format (cl_wilson.h:22-25, cl_wilson.cpp:110-288): the workStatus header,
 // then one (s0, s1) pair per test prime, the running products in the
 // reference's Montgomery form (R = 2^64 mod p^2, base-p digits), and the
-// additive state_sum; stateA.ckp and stateB.ckp written alternately.
+// additive state_sum; two files written alternately.
+//
+// Which files the two programs can share.  Below 2^32 both programs multiply
+// in exact primes.  From 2^32 on the reference multiplies in every base-2
+// strong probable prime that passes its 7..113 presieve (getsegprps.cl:211-293)
+// and divides the pseudoprimes among them (prps.dat) out of each row at the
+// very end, whatever its checkpoint's currp (cl_wilson.cpp:709-726); this
+// engine's columns above 2^32 are exact primes.  So a checkpoint whose columns
+// stop at currp <= 2^32 means the same thing to both programs, and one past
+// 2^32 does not: a reference file past 2^32 holds pseudoprime factors this
+// program never removes, and a file of this program past 2^32 lacks factors
+// that the reference would divide out.  Therefore:
+//   * checkpoints with currp <= 2^32, and finished ones, use the reference's
+//     names stateA.ckp / stateB.ckp;
+//   * checkpoints past 2^32 go to this program's own stateA.b200.ckp /
+//     stateB.b200.ckp, which the reference never reads;
+//   * a reference-named file past 2^32 that is not finished is refused
+//     (read_state returns 3) instead of being resumed with a wrong product.
 // Host code only (no CUDA).
 #pragma once
 #include <cstdint>
@@ -11,6 +28,11 @@
 
 static const char* const STATE_FILENAME_A = "stateA.ckp";
 static const char* const STATE_FILENAME_B = "stateB.ckp";
+static const char* const OWN_STATE_FILENAME_A = "stateA.b200.ckp";
+static const char* const OWN_STATE_FILENAME_B = "stateB.b200.ckp";
+// Largest currp whose running products mean the same to the reference and to
+// this program (columns q < currp, all below 2^32).
+static const uint64_t CKPT_SHARED_CURRP = 1ull << 32;
 
 typedef unsigned __int128 u128;
 
@@ -49,10 +71,14 @@ inline uint64_t state_checksum(const WorkStatus& st, const std::vector<uint64_t>
     return sum;
 }
 
-// write_state: the header then tpcount residue pairs, alternating A and B
+// write_state: the header then tpcount residue pairs, alternating A and B; the
+// reference's file names up to currp = 2^32 and for a finished workunit, this
+// program's own names past 2^32
 inline void write_state(bool& write_a_next, WorkStatus& st, const std::vector<uint64_t>& ref_res) {
     st.state_sum = state_checksum(st, ref_res);
-    const char* name = write_a_next ? STATE_FILENAME_A : STATE_FILENAME_B;
+    const bool shared = st.done || st.currp <= CKPT_SHARED_CURRP;
+    const char* name = write_a_next ? (shared ? STATE_FILENAME_A : OWN_STATE_FILENAME_A)
+                                    : (shared ? STATE_FILENAME_B : OWN_STATE_FILENAME_B);
     FILE* out = fopen(name, "wb");
     if (!out) {
         fprintf(stderr, "Cannot open %s !!!\n", name);
@@ -89,25 +115,36 @@ inline int read_one_state(const char* name, const WorkStatus& want, WorkStatus& 
     return r;
 }
 
+// read_state: 0 no usable checkpoint, 1 resume (st, ref_res filled), 2
+// finished, 3 refused (a reference-named file past 2^32, see the top)
 inline int read_state(bool& write_a_next, WorkStatus& st, std::vector<uint64_t>& ref_res) {
-    WorkStatus a, b;
-    std::vector<uint64_t> ra, rb;
-    const int ga = read_one_state(STATE_FILENAME_A, st, a, ra);
-    if (ga == 2) return 2;
-    const int gb = read_one_state(STATE_FILENAME_B, st, b, rb);
-    if (gb == 2) return 2;
-    if (ga == 1 && (gb != 1 || a.currp > b.currp)) {
-        st = a;
-        ref_res.swap(ra);
-        write_a_next = false;
-        return 1;
+    const char* names[4] = { STATE_FILENAME_A, STATE_FILENAME_B, OWN_STATE_FILENAME_A, OWN_STATE_FILENAME_B };
+    WorkStatus got[4];
+    std::vector<uint64_t> res[4];
+    int status[4];
+    for (int i = 0; i < 4; ++i) {
+        status[i] = read_one_state(names[i], st, got[i], res[i]);
+        if (status[i] == 2) return 2;
     }
-    if (gb == 1) {
-        st = b;
-        ref_res.swap(rb);
-        write_a_next = true;
-        return 1;
+    for (int i = 0; i < 2; ++i) {
+        if (status[i] == 1 && got[i].currp > CKPT_SHARED_CURRP) {
+            fprintf(stderr, "Checkpoint %s stops at P %llu, past 2^32, where its running products hold base-2 "
+                    "pseudoprime factors that only the reference program removes; finish this range with that "
+                    "program, or delete %s and %s to start over.\n", names[i], (unsigned long long)got[i].currp,
+                    STATE_FILENAME_A, STATE_FILENAME_B);
+            printf("Checkpoint %s stops at P %llu, past 2^32, where its running products hold base-2 "
+                   "pseudoprime factors that only the reference program removes; finish this range with that "
+                   "program, or delete %s and %s to start over.\n", names[i], (unsigned long long)got[i].currp,
+                   STATE_FILENAME_A, STATE_FILENAME_B);
+            return 3;
+        }
     }
-    return 0;
+    int best = -1;
+    for (int i = 0; i < 4; ++i)
+        if (status[i] == 1 && (best < 0 || got[i].currp > got[best].currp)) best = i;
+    if (best < 0) return 0;
+    st = got[best];
+    ref_res.swap(res[best]);
+    write_a_next = (best % 2) == 1;   // the other file of the pair is written next
+    return 1;
 }
-

@@ -12,7 +12,8 @@
 // line) exactly as the reference does.  Long searches run in pieces of columns and
 // checkpoint every minute to stateA.ckp / stateB.ckp in the reference's format
 // (cl_wilson.cpp:110-288), so a search resumes from its last checkpoint -- also one
-// written by the reference program.  All arithmetic runs in libwilson.so.
+// written by the reference program while its columns were below 2^32 (past
+// that point the two programs' running products differ; see wl_ckpt.h).  All arithmetic runs in libwilson.so.
 #include <getopt.h>
 #include <algorithm>
 #include <cinttypes>
@@ -247,6 +248,7 @@ static int search(wl_ctx* ctx, const Opts& o) {
     for (size_t i = 0; i < n; ++i) { res[2 * i] = 1; res[2 * i + 1] = 0; }
     bool write_a_next = true;
     const int rsr = read_state(write_a_next, ws, ref);
+    if (rsr == 3) return EXIT_FAILURE;   // a reference checkpoint past 2^32 (message printed)
     if (rsr == 2) {
         printf("Workunit complete.\n");
         fprintf(stderr, "Workunit complete.\n");
@@ -322,7 +324,9 @@ static int search(wl_ctx* ctx, const Opts& o) {
         printf("error: %s\n", wl_strerror(rr.rc));
         return EXIT_FAILURE;
     }
+    // result lines go to stdout too, except when verifying (cl_wilson.cpp:876-891)
     for (const wl_result& r : rr.results) {
+        if (o.result_test) break;
         if (r.value == 0) printf("%" PRIu64 " is a Wilson prime\n", r.p);
         else printf("%" PRIu64 " is a Near-Wilson prime %+d\n", r.p, r.value);
     }

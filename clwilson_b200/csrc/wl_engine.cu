@@ -104,6 +104,10 @@ int ensure_columns(wl_ctx* c, uint64_t limit) {
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
     c->ms_sieve += ms;
+    c->sieve_ints += nl;
+    // bitmap written, then read by the write-out; segment counts written and
+    // read; offsets written and read; the column table written
+    c->sieve_bytes += 2ull * nseg * SEG_WORDS * 4 + 2ull * nseg * 4 + 2ull * (nseg + 1) * 8 + total * 4;
     c->ncols = total;
     c->col_limit = nl;
     return 0;
@@ -399,6 +403,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     c->launches = 0;
     c->h2d = c->d2h = 0;
     c->ms_sieve = 0;
+    c->sieve_ints = c->sieve_bytes = 0;
     c->ms_big = 0;
     for (size_t i = 0; i < nr; ++i) RC(wl_check_range(ranges[i].pmin, ranges[i].pmax));
 
@@ -733,6 +738,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     }
     launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
     c->launches++;
+    RC(ensure(c->work, 24));
+    CK(cudaMemsetAsync(c->work.p, 0, 24, c->st));
     CK(cudaEventRecord(c->rows_ready, c->st));
     cudaEventRecord(c->ev[2], c->st);
     size_t ioff = 0;
@@ -747,7 +754,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(c->rowmod), as<uint32_t>(c->cols), as<uint32_t>(c->dsplit),
                                as<uint4>(c->part), as<Deficit>(c->defs), c->st2, c->tune.dense_kernel[g.L - 2],
-                               (uint32_t)c->tune.dense_hstep[g.L - 2]);
+                               (uint32_t)c->tune.dense_hstep[g.L - 2], as<unsigned long long>(c->work));
         else
             launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
                          as<SweepItem>(c->items) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->cols),
@@ -820,6 +827,9 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     std::vector<RowOut> ro(nrows);
     CK(cudaMemcpyAsync(ro.data(), c->rowout.p, (size_t)nrows * sizeof(RowOut), cudaMemcpyDeviceToHost, c->st));
     c->d2h += (size_t)nrows * sizeof(RowOut);
+    unsigned long long dwork[3] = { 0, 0, 0 };
+    CK(cudaMemcpyAsync(dwork, c->work.p, 24, cudaMemcpyDeviceToHost, c->st));
+    c->d2h += 24;
     cudaEventRecord(c->ev[5], c->st);
     CK(cudaStreamSynchronize(c->st));
     CK(cudaGetLastError());
@@ -864,6 +874,11 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         st->h2d_bytes = c->h2d;
         st->d2h_bytes = c->d2h;
         st->ms_big = c->ms_big;
+        st->sieve_integers = c->sieve_ints;
+        st->sieve_bytes = c->sieve_bytes;
+        st->dense_column_cells = dwork[0];
+        st->dense_window_cells = dwork[1];
+        st->dense_products = dwork[2];
     }
     return 0;
 }
@@ -1002,7 +1017,7 @@ void wl_close(wl_ctx* c) {
                        &c->buckets, &c->rowinfo, &c->rowmod, &c->items, &c->part, &c->ipart, &c->dsplit,
                        &c->bbitmap, &c->bsegcount, &c->boffsets, &c->boffs, &c->wcols, &c->wbuckets, &c->witems,
                        &c->wpart, &c->wdefs, &c->bacc, &c->bdef, &c->wkeys, &c->wcounts, &c->uacc, &c->udef,
-                       &c->defs, &c->rowout, &c->prod, &c->windesc, &c->seglo };
+                       &c->defs, &c->rowout, &c->prod, &c->windesc, &c->seglo, &c->work };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->fork) cudaEventDestroy(c->fork);
@@ -1241,65 +1256,43 @@ int wl_autotune(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, uin
     return 0;
 }
 
-// parse_uint64 (putil.c:34-116): decimal/hex/octal with K,M,G,T,P (x1000),
-// e<n> (x10^n), k,m,g,t,p (x2^10) and b<n> (x2^n) suffixes.
+// The reference CLI's number syntax (putil.c:34-116): an integer in C
+// notation (decimal, 0x.. hex, 0.. octal) and at most one scale suffix --
+// K M G T P (powers of 1000), k m g t p (powers of 1024), e<n> / E<n> (10^n),
+// b<n> / B<n> (2^n).  Returns 0, -1 (not a number of that form) or -2 (outside
+// [lo, hi], or overflow while scaling).
 int wl_parse_uint64(uint64_t* result, const char* str, uint64_t lo, uint64_t hi) {
     if (!result || !str) return -1;
+    struct Suffix { char c; uint64_t base; unsigned count; };   // count 0: the count follows the letter
+    static const Suffix suffixes[] = {
+        { 'K', 1000, 1 }, { 'M', 1000, 2 }, { 'G', 1000, 3 }, { 'T', 1000, 4 }, { 'P', 1000, 5 },
+        { 'k', 1024, 1 }, { 'm', 1024, 2 }, { 'g', 1024, 3 }, { 't', 1024, 4 }, { 'p', 1024, 5 },
+        { 'e', 10, 0 },   { 'E', 10, 0 },   { 'b', 2, 0 },    { 'B', 2, 0 },
+    };
     errno = 0;
-    char* tail = nullptr;
-    uint64_t num = strtoull(str, &tail, 0);
-    if (errno != 0 || num > hi) return -2;
-    uint32_t expt = 0;
-    switch (*tail) {
-        case 'P': expt += 3; [[fallthrough]];
-        case 'T': expt += 3; [[fallthrough]];
-        case 'G': expt += 3; [[fallthrough]];
-        case 'M': expt += 3; [[fallthrough]];
-        case 'K':
-            expt += 3;
-            if (tail[1] != '\0') return -1;
-            for (; expt > 0; expt -= 3) {
-                if (num > hi / 1000) return -2;
-                num *= 1000;
-            }
-            break;
-        case 'e':
-        case 'E':
-            expt = (uint32_t)strtoul(tail + 1, &tail, 0);
+    char* rest = nullptr;
+    uint64_t value = strtoull(str, &rest, 0);
+    if (errno != 0 || value > hi) return -2;
+    if (*rest != '\0') {
+        const Suffix* sx = nullptr;
+        for (const Suffix& x : suffixes)
+            if (x.c == *rest) sx = &x;
+        if (!sx) return -1;
+        unsigned long times = sx->count;
+        if (times == 0) {
+            times = strtoul(rest + 1, &rest, 0);
             if (errno != 0) return -2;
-            if (*tail != '\0') return -1;
-            while (expt-- > 0) {
-                if (num > hi / 10) return -2;
-                num *= 10;
-            }
-            break;
-        case 'p': expt += 10; [[fallthrough]];
-        case 't': expt += 10; [[fallthrough]];
-        case 'g': expt += 10; [[fallthrough]];
-        case 'm': expt += 10; [[fallthrough]];
-        case 'k':
-            expt += 10;
-            if (tail[1] != '\0') return -1;
-            if (num > (hi >> expt)) return -2;
-            num <<= expt;
-            break;
-        case 'b':
-        case 'B':
-            expt = (uint32_t)strtoul(tail + 1, &tail, 0);
-            if (errno != 0) return -2;
-            if (*tail != '\0') return -1;
-            while (expt-- > 0) {
-                if (num > (hi >> 1)) return -2;
-                num <<= 1;
-            }
-            break;
-        case '\0':
-            break;
-        default:
-            return -1;
+        } else {
+            ++rest;
+        }
+        if (*rest != '\0') return -1;
+        for (; times > 0 && value != 0; --times) {
+            if (value > hi / sx->base) return -2;
+            value *= sx->base;
+        }
     }
-    if (num < lo) return -2;
-    *result = num;
+    if (value < lo) return -2;
+    *result = value;
     return 0;
 }
 

@@ -90,6 +90,8 @@ struct wl_ctx {
     uint32_t launches = 0;
     uint64_t h2d = 0, d2h = 0;
     double ms_sieve = 0;
+    uint64_t sieve_ints = 0, sieve_bytes = 0;
+    DevBuf work;         // dense sweep work counters: column cells, window cells, products
 };
 
 // A range's window of test primes and its classes.

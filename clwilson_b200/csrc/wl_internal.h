@@ -139,9 +139,10 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
 // windows with the buckets in shared memory (3-bit at 4 CTAs/SM, 4-bit at 2)
 enum { DENSE_SORTED_W3 = 0, DENSE_SORTED_W4 = 1, DENSE_SWITCH_W3 = 2, DENSE_SWITCH_W4 = 3, DENSE_SMEM_W3 = 4,
        DENSE_SMEM_W4 = 5 };
+// work (may be null): adds the launch's column cells, window cells and full products, summed over rows
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
-                        cudaStream_t st, int kernel, uint32_t hstep);
+                        cudaStream_t st, int kernel, uint32_t hstep, unsigned long long* work = nullptr);
 void launch_sieve_big(uint64_t lo, uint64_t hi, uint32_t nseg, uint32_t segs_per_cta, const uint32_t* base,
                       uint32_t nbase, uint32_t* offsets, uint32_t* bitmap, uint32_t* seg_count, cudaStream_t st);
 void launch_compact_big(uint32_t nseg, uint64_t lo0, const uint32_t* bitmap, const uint64_t* offsets, uint64_t* out,

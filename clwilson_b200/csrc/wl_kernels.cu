@@ -499,11 +499,18 @@ constexpr uint32_t DENSE_GMAX = 32;   // splits per CTA at most (tps >= 8)
 // memory (bucket d of thread t at sbk[d * 256 + t]); a digit's run loads its
 // bucket once, runs its cells in registers and stores it back.  That frees the
 // bucket registers (more CTAs per SM, or wider windows).
+//
+// work (optional): the launch's work summed over rows -- work[0] += cells of
+// the exponent's high part (one per column), work[1] += cells of the window
+// digits, work[2] += full Montgomery products (about L cells each).  Every
+// thread of a group runs the same sequence, so its first thread adds the
+// group's counts times its rows.
 template <int L, int MINB, int DW, int RPT, int SORT, int SMB = 0>
 __global__ void __launch_bounds__(256, MINB)
 k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
               const RowMod* __restrict__ mods, const uint32_t* __restrict__ cols, const uint32_t* __restrict__ dsplit,
-              uint4* __restrict__ part, Deficit* __restrict__ defs, uint32_t hstep) {
+              uint4* __restrict__ part, Deficit* __restrict__ defs, uint32_t hstep,
+              unsigned long long* __restrict__ work) {
     __shared__ uint32_t sq[DENSE_CHUNK];
     __shared__ uint64_t sm[DENSE_CHUNK];
     __shared__ uint32_t ss[SORT ? DENSE_CHUNK : 1];       // chunk sorted by digit
@@ -571,6 +578,7 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     u128 defA = 0;
     uint64_t h_cur = e_first >> sb;
     uint32_t cells = 0;
+    uint64_t nprod = 0, nbucket = 0;   // work counters (full products; window cells)
     for (uint32_t ch = 0; ch < nchunks; ++ch) {
         __syncthreads();
         const uint64_t cb = c0 + (uint64_t)ch * KG;
@@ -590,6 +598,7 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], d, n[j], ninv[j]);
                 defA += (u128)d * (32ull * cells + 32 * L);
+                nprod += (uint64_t)(63 - __clzll((long long)d)) + __popcll(d);
                 h_cur = h;
             }
             const uint32_t q = sq[base + k];
@@ -606,12 +615,14 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
 #pragma unroll
         for (int j = 0; j < RPT; ++j) fold_pow<L>(A[j], P[j], h_cur, n[j], ninv[j]);
         defA += (u128)h_cur * (32ull * cells + 32 * L);
+        nprod += (uint64_t)(63 - __clzll((long long)h_cur)) + __popcll(h_cur);
     }
     for (uint32_t k = 0; k < sb; ++k) {               // A^(2^sb)
 #pragma unroll
         for (int j = 0; j < RPT; ++j) A[j] = mont_mul<L>(A[j], A[j], n[j], ninv[j]);
         defA = 2 * defA + 32 * L;
     }
+    nprod += sb;
 
     // ---- windows over the low bits, top window first ----
     Res<L> acc[RPT];
@@ -674,6 +685,8 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
 #pragma unroll
                 for (int d = 1; d <= NBK; ++d) {
                     const uint32_t k0 = scur[g][d - 1], k1 = scur[g][d];
+                    nbucket += k1 - k0;
+                    nprod += (k1 - k0 >= 2) ? 1u : 0u;
                     if (SMB) {
                         if (k1 == k0) continue;
                         const uint4 v = sbk[(d - 1) * 256 + threadIdx.x];
@@ -721,6 +734,7 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
                     if constexpr (!SMB) {
                         if (d) bucket_cell<L, NBK, RPT>(B, d, q, n, ninv, L != 2 && q >= 0x80000000u);
                     }
+                    nbucket += d ? 1u : 0u;
                 }
             }
         }
@@ -762,6 +776,7 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
             for (int k = 0; k < DW; ++k) defacc = 2 * defacc + 32 * L;
             defacc += defR + 32 * L;
         }
+        nprod += 2 * (NBK - 1) + (w == (int)nwin - 1 ? 0 : DW + 1);
     }
     u128 def = defA;
     if (nwin) def = defA + defacc + 32 * L;
@@ -783,6 +798,14 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
         dd.lo = (uint64_t)def;
         dd.hi = (uint64_t)(def >> 64);
         defs[bk.def_base + s] = dd;
+    }
+    if (work && has_split && lt == 0) {
+        const uint32_t left = bk.nrows > it.row0 ? bk.nrows - it.row0 : 0u;
+        const uint64_t rows = left < tps * RPT ? left : tps * RPT;
+        if (nwin) ++nprod;                              // A * acc
+        atomicAdd(&work[0], (unsigned long long)(cells * rows));
+        atomicAdd(&work[1], (unsigned long long)(nbucket * rows));
+        atomicAdd(&work[2], (unsigned long long)(nprod * rows));
     }
 }
 
@@ -884,12 +907,21 @@ __device__ bool cornacchia(uint64_t p, uint64_t d, uint64_t r0, uint64_t* x, uin
     return true;
 }
 
+// The search for a non-residue g (quadratic for find_a, cubic for find_cu)
+// runs to this bound, then reports "no representation".  Under the
+// generalised Riemann hypothesis the least non-residue of either kind is
+// below 3 (ln p)^2 < 6,000 for p < 2^62 (Bach's explicit bound); among the
+// primes below 1e8 the largest least cubic non-residue is 41 (p = 65139031).
+// For type 1 (p = 5 mod 12) the quadratic search ends at g = 2 or 3, since
+// (3/p) = (p/3) = -1 there.
+constexpr uint64_t NONRESIDUE_LIMIT = 1ull << 16;
+
 // a with p = a^2 + b^2 (a odd, sign a = 1 mod 4: find.cl:52-58, only a^2 is used)
 __device__ bool find_a(uint64_t p, int64_t* out) {
     Mod64 M;
     M.init(p);
     const uint64_t minus1 = p - 1;
-    for (uint64_t g = 2; g < 200; ++g) {
+    for (uint64_t g = 2; g < NONRESIDUE_LIMIT && g < p; ++g) {
         if (M.from(M.pow(M.to(g), (p - 1) / 2)) != minus1) continue;
         const uint64_t r = M.from(M.pow(M.to(g), (p - 1) / 4));
         uint64_t x, y;
@@ -906,7 +938,7 @@ __device__ bool find_a(uint64_t p, int64_t* out) {
 __device__ bool find_cu(uint64_t p, int64_t* c_out, int64_t* u_out) {
     Mod64 M;
     M.init(p);
-    for (uint64_t g = 2; g < 200; ++g) {
+    for (uint64_t g = 2; g < NONRESIDUE_LIMIT && g < p; ++g) {
         const uint64_t w = M.from(M.pow(M.to(g), (p - 1) / 3));
         if (w == 1) continue;
         const uint64_t r = (2 * w + 1) % p;            // sqrt(-3) mod p
@@ -1764,11 +1796,12 @@ void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* bu
 }
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,
-                        cudaStream_t st, int kernel, uint32_t hstep) {
+                        cudaStream_t st, int kernel, uint32_t hstep, unsigned long long* work) {
     if (!nitems) return;
     if (hstep == 0) hstep = 8;
 #define WL_D(LL, MB, DWB, RR, SS) \
-    k_sweep_dense<LL, MB, DWB, RR, SS><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs, hstep)
+    k_sweep_dense<LL, MB, DWB, RR, SS><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, dsplit, part, defs, hstep, \
+                                                                work)
 #define WL_DS(LL, MB, DWB) do {                                                                   \
         constexpr int nbk_ = (1 << DWB) - 1;                                                           \
         const int smem_ = nbk_ * 256 * (int)sizeof(uint4);                                             \
@@ -1779,7 +1812,7 @@ void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, 
             attr_ = true;                                                                               \
         }                                                                                               \
         k_sweep_dense<LL, MB, DWB, 1, 1, 1><<<nitems, 256, smem_, st>>>(buckets, items, mods, cols, dsplit, \
-                                                                      part, defs, hstep);               \
+                                                                      part, defs, hstep, work);         \
     } while (0)
     if (rpt == 2) {
         if (L == 2) WL_D(2, 2, 3, 2, 0); else if (L == 3) WL_D(3, 2, 3, 2, 0); else WL_D(4, 2, 3, 2, 0);

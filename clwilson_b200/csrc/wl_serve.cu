@@ -332,7 +332,14 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
 }
 
 // One scheduler step: every bucket with columns left advances by one chunk.
+static int serve_step_run(wl_server* s);
 static int serve_step(wl_server* s) {
+    const double t = s->now_ms();
+    const int e = serve_step_run(s);
+    s->ws.ms_wall_steps += s->now_ms() - t;
+    return e;
+}
+static int serve_step_run(wl_server* s) {
     wl_ctx* c = s->c;
     struct Work { uint32_t bid; uint64_t c0, len; bool dense; };
     std::vector<Work> work;
@@ -475,7 +482,14 @@ static int serve_step(wl_server* s) {
     return 0;
 }
 
+static int serve_finish_run(wl_server* s, SReq* q);
 static int serve_finish(wl_server* s, SReq* q) {
+    const double t = s->now_ms();
+    const int e = serve_finish_run(s, q);
+    s->ws.ms_wall_finish += s->now_ms() - t;
+    return e;
+}
+static int serve_finish_run(wl_server* s, SReq* q) {
     wl_ctx* c = s->c;
     const bool full = q->qcap == 0;
     launch_finish(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), nullptr, nullptr, 1,
@@ -554,7 +568,9 @@ static void serve_loop(wl_server* s) {
         }
         if (!cands.empty()) {
             std::vector<int> res;
+            const double t = s->now_ms();
             serve_admit_batch(s, cands, res);
+            s->ws.ms_wall_admit += s->now_ms() - t;
             std::lock_guard<std::mutex> lk(s->mu);
             for (size_t k = 0; k < cands.size(); ++k) {
                 SReq* q = cands[k];

@@ -113,6 +113,15 @@ typedef struct {
     double ms_finish;           /* combine + lift */
     uint64_t h2d_bytes, d2h_bytes;
     double ms_big;              /* columns above 2^32 (window sieve + sweep + merge), own stream */
+    uint64_t sieve_integers;    /* integers the column sieve covered (0 when the cache already held them) */
+    uint64_t sieve_bytes;       /* its device-memory traffic: bitmap written and read back, counts,
+                                   offsets, the column table written (4 B per prime) */
+    uint64_t dense_column_cells; /* cells of the dense-regime sweep for the exponent's high part,
+                                    one per (row, column); included in `cells` */
+    uint64_t dense_window_cells; /* its further cells, one per nonzero window digit of the
+                                    exponent's low part, summed over rows */
+    uint64_t dense_products;    /* full Montgomery products it executed, summed over rows (about
+                                   L cells each) */
 } wl_stats;
 
 /* Open a context on CUDA device `device`. */
@@ -190,15 +199,22 @@ void wl_drop_columns(wl_ctx *ctx);
  *   s0s1    device array of 2 * nrows uint64_t (output)
  *   stream  the cudaStream_t to run on (NULL: the legacy default stream); the
  *           call returns once the work is queued, like a kernel launch
+ * The inputs are checked on the device: a row whose prime is even, below 5
+ * or not below p_bound gets s0 = s1 = UINT64_MAX (a real digit is < p), and
+ * so does every row when a column is below 2, above T or not above the one
+ * before it.  A CUDA error already pending in the calling thread is returned
+ * as WL_ERR_CUDA before anything is launched (and left pending); a launch
+ * that fails returns WL_ERR_CUDA at once.
  * All intermediate data lives in one fixed array of WL_NOALLOC_SCRATCH_BYTES
  * (5 MiB) of device memory that the CUDA runtime places on every GPU that
  * loads the library and keeps until the process exits.  Limits: nrows <=
  * WL_NOALLOC_MAX_ROWS and (column splits x nrows) <= WL_NOALLOC_MAX_PARTIALS;
  * larger requests return WL_ERR_TOO_LARGE.  The call uses the current CUDA
  * device; its first call on a device resolves the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * Calls share the array and each call overwrites everything it reads before
- * reading it (nothing has to start at zero); calls that overlap on the GPU
+ * (cudaGetSymbolAddress, once per device under a lock, so first calls from
+ * several host threads are safe), so make that first call before any stream
+ * capture.  Calls share the array; each call clears the one word that must
+ * start at zero and overwrites everything else it reads before reading it; calls that overlap on the GPU
  * (different streams, or another host thread) race on it and must be
  * serialised by the caller. */
 #define WL_NOALLOC_MAX_ROWS      4096u
@@ -301,6 +317,9 @@ typedef struct {
     double ms_admit;       /* device time of admissions */
     uint32_t peak_rows;    /* largest number of resident rows */
     uint32_t peak_active;  /* largest number of admitted requests at once */
+    double ms_wall_steps;  /* scheduler wall time in steps: planning, uploads, launches, waiting */
+    double ms_wall_admit;  /* scheduler wall time in admissions */
+    double ms_wall_finish; /* scheduler wall time finishing requests (lift, read-back, result lines) */
 } wl_server_stats;
 
 int wl_server_open(const wl_server_opts *opts, wl_server **out);

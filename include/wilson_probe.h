@@ -18,11 +18,6 @@ extern "C" {
 #define WL_PROBE_CELL3  3   /* sweep cells per second, 3-limb residues (p < 2^47) */
 #define WL_PROBE_CELL4  4   /* sweep cells per second, 4-limb residues (p < 2^62) */
 #define WL_PROBE_MADWIDE 5  /* mad.wide.u32 operations per second */
-#define WL_PROBE_DFMA    6  /* fma.rn.f64 operations per second */
-#define WL_PROBE_MAD_DFMA 7       /* mad.lo.u32 + fma.rn.f64 interleaved: operations of both kinds per second */
-#define WL_PROBE_MADWIDE_DFMA 8   /* mad.wide.u32 + fma.rn.f64 interleaved: operations of both kinds per second */
-#define WL_PROBE_CELL2_FP64 9     /* exact 2-limb Montgomery cells in FP64 per second */
-#define WL_PROBE_CELL2_MIX 10     /* integer cells (6 warps of 8) + FP64 cells (2 warps) per second */
 /* 100 + 10*(L-2) + v: cell formulation v (0 carry-flag chain, 1 wide
    products, 2 wide products with a high-half first reduction) at width L */
 

@@ -278,7 +278,7 @@ static int cornacchia(u64 p, u64 d, u64 r0, u64 *x, u64 *y) {
 }
 /* a with p = a^2 + b^2, a = 1 (mod 4), for p = 1 (mod 4) */
 int orc_cornacchia_a(u64 p, int64_t *out) {
-    for (u64 g = 2; g < 1000; ++g) {
+    for (u64 g = 2; g < (1u << 16) && g < p; ++g) {
         if (powmod64(g, (p - 1) / 2, p) != p - 1) continue;   /* g non-residue */
         u64 r = powmod64(g, (p - 1) / 4, p), x, y;             /* r^2 = -1 */
         if (cornacchia(p, 1, r, &x, &y)) return -1;
@@ -291,7 +291,7 @@ int orc_cornacchia_a(u64 p, int64_t *out) {
 /* c with 4p = c^2 + 27 d^2 (c = 1 mod 3) and one u with 4p = u^2 + 3 v^2
    (u = umod mod 3), for p = 1 (mod 3) */
 int orc_cornacchia_cu(u64 p, int64_t *c_out, int64_t *u_out) {
-    for (u64 g = 2; g < 1000; ++g) {
+    for (u64 g = 2; g < (1u << 16) && g < p; ++g) {
         u64 w = powmod64(g, (p - 1) / 3, p);                   /* cube root of 1 */
         if (w == 1) continue;
         u64 r = (2 * w + 1) % p;                               /* r^2 = -3 */

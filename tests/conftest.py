@@ -25,7 +25,7 @@ def golden():
     import json
     d = os.path.join(ROOT, "tests", "golden")
     out = {}
-    for name in ("kat", "small", "range_1e5", "capped"):
+    for name in ("kat", "small", "range_1e5", "capped", "nonresidue"):
         with open(os.path.join(d, name + ".json")) as f:
             out[name] = json.load(f)
     return out

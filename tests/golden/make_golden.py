@@ -10,6 +10,9 @@ reference's built-in self-test, so the fixtures pin both independently.
   range_1e5.json   the full search of [100000, 101000): result lines, checksum
   capped.json      capped partial products prod_{q < Q, q <= T} q^{v_q(T!)} mod p^2
                    for test primes of the mid-size and top-of-range workloads
+  nonresidue.json  the primes p = 1 mod 3 below 1e8 whose least cubic non-residue
+                   is 37 or more (the lift's c and u come from a search for one),
+                   with (p-1)! + 1 mod p^2 as (rem, quot)
 
 Run:  python tests/golden/make_golden.py
 """
@@ -167,6 +170,27 @@ def capped(pmin: int, pmax: int, qcap: int, take: int):
             "rows": rows}
 
 
+def nonresidue(limit: int = 10 ** 8, least: int = 37):
+    sieve = bytearray([1]) * limit
+    sieve[0:2] = b"\x00\x00"
+    for i in range(2, int(limit ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = bytearray(len(sieve[i * i::i]))
+    gs = [g for g in range(2, 200) if sieve[g]]
+    rows = []
+    for p in range(7, limit, 6):          # p = 1 mod 6
+        if not sieve[p]:
+            continue
+        e = (p - 1) // 3
+        g = next(g for g in gs if pow(g, e, p) != 1)
+        if g < least:
+            continue
+        m = p * p
+        v = (fact_mod(p - 1, m) + 1) % m
+        rows.append({"p": p, "type": 0, "least_cubic_nonresidue": g, "rem": v % p, "quot": v // p})
+    return rows
+
+
 def main():
     def dump(name, obj):
         with open(os.path.join(HERE, name), "w") as f:
@@ -181,6 +205,7 @@ def main():
         capped((1 << 62) - 1 - 10 ** 7, (1 << 62) - 1, 1 << 16, 6),
         capped(4294967296 - 30000, 4294967296 + 30000, 1 << 16, 6),
     ])
+    dump("nonresidue.json", nonresidue())
 
 
 if __name__ == "__main__":

@@ -103,7 +103,8 @@ def _ref_parse(s, lo, hi):
 
 @pytest.mark.parametrize("text", ["5", "1000", "1e9", "1E3", "2K", "3M", "1G", "2T", "1P", "4k", "1m", "3g",
                                   "1b10", "0x10", "010", "12x", "1e", "5KK", "4611686018427387903",
-                                  "4611686018427387904", "99999999999999999999", "4", "1p", "abc", ""])
+                                  "4611686018427387904", "99999999999999999999", "4", "1p", "abc", "",
+                                  "0K", "7b0", "9e0", "5e18", "1b62", "3p", "0x1Fe3", "5Q", "12e1x", "6b"])
 def test_parse_uint64(text):
     lo, hi = 5, wl.WL_MAXP
     rc, v = wl.parse_uint64(text, lo, hi)

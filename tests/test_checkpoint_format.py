@@ -81,3 +81,39 @@ def test_newest_valid_file_wins(driver, tmp_path):
     # a finished workunit
     _run(driver, tmp_path, "write", "B", 200, 564, 400, 1, 0, 1, *_residues(2))
     assert _run(driver, tmp_path, "read", 200, 564, 2).splitlines()[-1].startswith("status 2")
+
+
+def test_files_past_2_32(driver, tmp_path):
+    # p ~ 1e10: the type-2 target (p-1)/2 is above 2^32, so a search checkpoints
+    # past 2^32, where the reference's running products hold base-2
+    # pseudoprime factors (cl_wilson.cpp:709-726) and this program's do not
+    lo, hi = 10**10, 10**10 + 200
+    past = (1 << 32) + 1001
+    # a file of this program past 2^32 goes to its own name, and resumes
+    out = _run(driver, tmp_path, "write", "A", lo, hi, past, 1, 0, 0, *_residues(2))
+    assert out.strip() == "next B"
+    assert (tmp_path / "stateA.b200.ckp").exists() and not (tmp_path / "stateA.ckp").exists()
+    out = _run(driver, tmp_path, "read", lo, hi, 2)
+    assert out.split()[:4] == ["status", "1", "currp", str(past)]
+    # a reference-named file at currp = 2^32 is shared by both programs
+    d2 = tmp_path / "shared"
+    d2.mkdir()
+    _run(driver, d2, "write", "B", lo, hi, 1 << 32, 1, 0, 0, *_residues(2))
+    assert (d2 / "stateB.ckp").exists()
+    out = _run(driver, d2, "read", lo, hi, 2)
+    assert out.split()[:4] == ["status", "1", "currp", str(1 << 32)]
+    # a reference-named file past 2^32 (as the reference writes it) is refused
+    # with a message, also when an older file of this program exists
+    data = bytearray((tmp_path / "stateA.b200.ckp").read_bytes())
+    pmin, pmax, currp, trickle, ssum, total, tpcount, done = struct.unpack(HDR, bytes(data[:56]))
+    currp2 = past + 10**6
+    ssum2 = (ssum - currp + currp2) % (1 << 64)
+    data[:56] = struct.pack(HDR, pmin, pmax, currp2, trickle, ssum2, total, tpcount, done)
+    (tmp_path / "stateB.ckp").write_bytes(bytes(data))
+    out = _run(driver, tmp_path, "read", lo, hi, 2)
+    assert "past 2^32" in out and "stateB.ckp" in out
+    assert out.splitlines()[-1].startswith("status 3")
+    # a finished workunit is reported whatever its currp
+    _run(driver, tmp_path, "write", "A", lo, hi, past + 5, 1, 0, 1, *_residues(2))
+    assert (tmp_path / "stateA.ckp").exists()
+    assert _run(driver, tmp_path, "read", lo, hi, 2).splitlines()[-1].startswith("status 2")

@@ -105,10 +105,13 @@ class OracleEngine:
         return rows, targets
 
     def rows_from(self, pmin, pmax, q_lo, q_cap=0, init=None):
-        assert q_cap > q_lo >= 2 and init is None
+        assert q_cap >= q_lo >= 2 and init is None
         rows, targets = self._class_targets(pmin, pmax)
         for r in rows:
-            r["s0"], r["s1"] = oracle.range_product(int(r["p"]), targets[int(r["type"])], q_lo, q_cap)
+            if q_cap == q_lo:                      # no column: the empty product
+                r["s0"], r["s1"] = 1, 0
+            else:
+                r["s0"], r["s1"] = oracle.range_product(int(r["p"]), targets[int(r["type"])], q_lo, q_cap)
         return rows, None
 
     def rows_product(self, parts, p=None):
@@ -141,7 +144,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, ranges, q, perturb=False):
+def _rank_main(rank, world, port, ranges, q, perturb=False, own_gather=False):
     import datetime
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -156,9 +159,17 @@ def _rank_main(rank, world, port, ranges, q, perturb=False):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         out = []
+        # a caller's gather: no broadcast of rank 0's boundaries, so with
+        # perturbed plans rank 0 must find the mismatch in the pieces' headers
+        gather = (lambda arr: cs.gather_to_rank0(arr, rank, world)) if own_gather else None
         for pmin, pmax in ranges:
             eng = OracleEngine()
-            res = cs.search_columns_sharded(eng, pmin, pmax, rank, world)
+            try:
+                res = cs.search_columns_sharded(eng, pmin, pmax, rank, world, gather=gather)
+            except ValueError as e:
+                assert rank == 0
+                out.append(("raised", str(e)))
+                continue
             out.append(None if res is None else (res.lines, res.checksum, eng.finished))
         if rank == 0:
             q.put(out)
@@ -182,3 +193,36 @@ def test_sharded_flow_matches_oracle(world, perturb):
         assert fin == colshard.column_end(pmax)
     # self-test case 5 (cl_wilson.cpp:2075-2081): 57 lines, checksum 00000000000080A3
     assert "%016X" % got[0][1] == "00000000000080A3" and len(got[0][0]) == 57
+
+
+@pytest.mark.parametrize("perturb", [False, True])
+def test_sharded_flow_with_own_gather(perturb):
+    # a caller-supplied gather (here the tensor gather, called directly):
+    # agreeing plans give the oracle's result; when the other ranks plan other
+    # boundaries, rank 0 refuses the pieces instead of multiplying them
+    world = 3
+    ranges = [(200, 564), (10**6, 10**6 + 3000)]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    mp.start_processes(_rank_main, args=(world, _free_port(), ranges, q, perturb, True), nprocs=world,
+                       start_method="spawn", join=True)
+    got = q.get(timeout=60)
+    for (pmin, pmax), r in zip(ranges, got):
+        if perturb:
+            assert r[0] == "raised" and "column pieces disagree" in r[1]
+        else:
+            full, _ = oracle.search(pmin, pmax)
+            assert r[0] == oracle.result_lines(full) and r[1] == oracle.checksum(full)
+
+
+def test_piece_headers():
+    b = [2, 100, 5000, 9001]
+    rows = np.zeros(3, dtype=oracle.ROW_DTYPE)
+    rows["s0"], rows["s1"] = [1, 2, 3], [4, 5, 6]
+    parts = [colshard.piece_digits(rows, colshard.piece_interval(b, r)) for r in range(4)]
+    assert parts[0].shape == (4, 2) and tuple(parts[0][0]) == (2, 100) and tuple(parts[3][0]) == (0, 0)
+    got = colshard.check_pieces(b, parts)
+    assert len(got) == 3 and all(np.array_equal(x[:, 0], [1, 2, 3]) for x in got)
+    parts[1][0, 1] += 1
+    with pytest.raises(ValueError):
+        colshard.check_pieces(b, parts)

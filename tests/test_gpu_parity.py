@@ -193,3 +193,22 @@ def test_kat1_columns_above_2_32(engine, golden):
     assert res.stats.pi_maxtarget == k["pi_maxtarget"]
     assert "%016X" % res.checksum == k["checksum"]
     assert res.results == [(k["last_prime"], k["last_value"])]
+
+
+def test_large_least_cubic_nonresidue(engine, golden):
+    # type-0 primes whose least cubic non-residue is 37 or 41 (the largest
+    # below 1e8): the lift's search for c and u (k_finish, find.cl:71-117)
+    # runs that far; exact (p-1)! + 1 mod p^2 from Python integers, and the
+    # oracle's rows; then all of them as ranges of one batch
+    ranges = []
+    for g in golden["nonresidue"]:
+        p = g["p"]
+        rows, _ = engine.rows(p, p + 1)
+        assert len(rows) == 1 and int(rows["status"][0]) == 0
+        assert (int(rows["rem"][0]), int(rows["quot"][0])) == (g["rem"], g["quot"]), p
+        want, _ = oracle.search(p, p + 1)
+        assert (int(rows["s0"][0]), int(rows["s1"][0])) == (int(want["s0"][0]), int(want["s1"][0])), p
+        ranges.append((p, p + 1))
+    per, _, _ = engine.batch(ranges)
+    for (p, _), pr, g in zip(ranges, per, golden["nonresidue"]):
+        assert pr["checksum"] == (p + g["rem"] + g["quot"]) % (1 << 64) and pr["status"] == 0

@@ -133,3 +133,20 @@ def test_primality_against_sieve():
         sieve[start - lo::q] = False
     want = np.nonzero(sieve)[0] + lo
     assert np.array_equal(got, want.astype(np.uint64))
+
+
+def test_large_least_cubic_nonresidue(golden):
+    # primes whose least cubic non-residue is 37 or 41, the largest below 1e8:
+    # the lift's search for c and u runs that far; (p-1)! + 1 mod p^2 from exact
+    # integers, and Cornacchia's c equal to the reference's brute-force one
+    # (find.cl:71-92); any u with 4p = u^2 + 3v^2 and the sign rule works
+    assert len(golden["nonresidue"]) == 8
+    for g in golden["nonresidue"]:
+        p = g["p"]
+        assert all(pow(k, (p - 1) // 3, p) == 1 for k in range(2, g["least_cubic_nonresidue"]))
+        c, u = oracle.cornacchia_cu(p)
+        assert c == oracle.find_c_brute(p)
+        v2 = (4 * p - u * u) // 3
+        assert 3 * v2 + u * u == 4 * p and int(round(v2 ** 0.5)) ** 2 == v2
+        rows, _ = oracle.search(p, p + 1)
+        assert (int(rows[0]["rem"]), int(rows[0]["quot"])) == (g["rem"], g["quot"]) and int(rows[0]["status"]) == 0

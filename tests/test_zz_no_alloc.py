@@ -77,3 +77,55 @@ def test_noalloc_top_of_range_and_limits(engine):
     rc, _ = _noalloc(L, too_many, 2 * 10**6, 10**5, cols[:10])
     assert rc == -9
     assert L.wl_strerror(rc) != b"unknown error"
+
+
+def test_noalloc_no_columns_and_full_rows(engine):
+    L = wl.load_library()
+    # no columns: an empty product (1 = s0 + p*s1 with s0 = 1, s1 = 0), as
+    # wl_rows gives with q_cap = 2
+    lo, hi = 10**9, 10**9 + 200000
+    rows0, st0 = engine.rows(lo, hi, q_cap=2)
+    sel0 = rows0[rows0["type"] == 0][:300]
+    rc, got = _noalloc(L, sel0["p"], hi, st0.targets[0], np.zeros(0, dtype=np.uint32))
+    assert rc == 0
+    assert np.array_equal(got[:, 0], sel0["s0"]) and np.array_equal(got[:, 1], sel0["s1"])
+    assert (got[:, 0] == 1).all() and (got[:, 1] == 0).all()
+    # the largest row count the scratch holds: the split count is clipped by
+    # the partial-product region, which is then fullest
+    rows, st = engine.rows(lo, hi, q_cap=QCAP)
+    T = st.targets[0]
+    sel = rows[rows["type"] == 0][:4096]
+    assert len(sel) == 4096
+    allq = _primes_below(QCAP)
+    cols = allq[allq <= T]
+    rc, got = _noalloc(L, sel["p"], hi, T, cols)
+    assert rc == 0
+    assert np.array_equal(got[:, 0], sel["s0"]) and np.array_equal(got[:, 1], sel["s1"])
+
+
+def test_noalloc_flags_inputs_that_break_the_contract(engine):
+    L = wl.load_library()
+    lo, hi = 10**9, 10**9 + 20000
+    rows, st = engine.rows(lo, hi, q_cap=QCAP)
+    T = st.targets[0]
+    sel = rows[rows["type"] == 0]
+    allq = _primes_below(QCAP)
+    cols = allq[allq <= T]
+    bad = np.array(sel["p"], dtype=np.uint64)
+    bad[3] = hi + 2          # not below p_bound
+    bad[5] = 1000000000      # even
+    rc, got = _noalloc(L, bad, hi, T, cols)
+    assert rc == 0
+    flagged = np.zeros(len(bad), dtype=bool)
+    flagged[[3, 5]] = True
+    assert (got[flagged] == np.uint64(0xFFFFFFFFFFFFFFFF)).all()
+    assert np.array_equal(got[~flagged, 0], sel["s0"][~flagged])
+    assert np.array_equal(got[~flagged, 1], sel["s1"][~flagged])
+    # columns out of order, or above T: every row is flagged
+    for cc in (cols[::-1].copy(), np.append(cols, np.uint32(T + 2))):
+        rc, got = _noalloc(L, sel["p"], hi, T, cc)
+        assert rc == 0
+        assert (got == np.uint64(0xFFFFFFFFFFFFFFFF)).all()
+    # and a correct call right after gives the rows again
+    rc, got = _noalloc(L, sel["p"], hi, T, cols)
+    assert rc == 0 and np.array_equal(got[:, 0], sel["s0"]) and np.array_equal(got[:, 1], sel["s1"])

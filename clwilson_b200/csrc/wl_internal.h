@@ -151,9 +151,10 @@ void launch_count_leq64(const uint64_t* cols, uint64_t ncols, const uint64_t* ke
                         cudaStream_t st);
 void launch_sweep64(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items, const RowMod* mods,
                     const uint64_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+// los (may be null): per-bucket bitmap regions, bucket b's at word cbase holding los[b] + 64w + 1 + 2i
 void launch_sweep_bits(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                        const RowMod* mods, const uint32_t* bitmap, uint64_t lo, const uint64_t* keys, uint4* part,
-                       Deficit* defs, cudaStream_t st);
+                       Deficit* defs, cudaStream_t st, const uint64_t* los = nullptr);
 void launch_count_bits(const uint32_t* bitmap, uint64_t lo, uint64_t nwords, uint64_t key, unsigned long long* out,
                        cudaStream_t st);
 void launch_merge(int L, const Bucket* buckets, const RowInfo* info, const RowMod* mods, const uint4* part,

@@ -1446,11 +1446,14 @@ k_sweep64(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ item
 // lo + 64w + 1 + 2b (bit b).  Bucket fields for the window: ncols = words used,
 // split s = words [ncols*s/nsplit, ncols*(s+1)/nsplit); primes above `key`
 // (the bucket's target or q_cap - 1) are skipped.  Otherwise as k_sweep64.
+// With los (serving, where buckets sit at different places of the number
+// line), each bucket has its own bitmap region: words from Bucket::cbase on,
+// word w of the region holding los[bucket] + 64w + 1 + 2b.
 template <int L, int RPT>
 __global__ void __launch_bounds__(256)
 k_sweep_bits(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
              const uint32_t* __restrict__ bitmap, uint64_t lo, const uint64_t* __restrict__ keys,
-             uint4* __restrict__ part, Deficit* __restrict__ defs) {
+             uint4* __restrict__ part, Deficit* __restrict__ defs, const uint64_t* __restrict__ los) {
     const SweepItem it = items[blockIdx.x];
     const Bucket bk = buckets[it.bucket];
     const uint32_t s = it.split0 + threadIdx.x / it.tps;
@@ -1471,6 +1474,10 @@ k_sweep_bits(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ i
     const uint64_t T = bk.T, key = keys[it.bucket];
     const uint64_t w0 = (uint64_t)bk.ncols * s / bk.nsplit;
     const uint64_t w1 = (uint64_t)bk.ncols * (s + 1) / bk.nsplit;
+    if (los) {
+        lo = los[it.bucket];
+        bitmap += bk.cbase;
+    }
     Res<L> P[RPT], A[RPT];
 #pragma unroll
     for (int j = 0; j < RPT; ++j) { set_small<L>(P[j], 1); set_small<L>(A[j], 1); }
@@ -1919,9 +1926,10 @@ void launch_tail_merge(int L, const Bucket* buckets, const RowInfo* info, const 
 }
 void launch_sweep_bits(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                        const RowMod* mods, const uint32_t* bitmap, uint64_t lo, const uint64_t* keys, uint4* part,
-                       Deficit* defs, cudaStream_t st) {
+                       Deficit* defs, cudaStream_t st, const uint64_t* los) {
     if (!nitems) return;
-#define WL_SB(LL, RR) k_sweep_bits<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, bitmap, lo, keys, part, defs)
+#define WL_SB(LL, RR) k_sweep_bits<LL, RR><<<nitems, 256, 0, st>>>(buckets, items, mods, bitmap, lo, keys, part, defs, \
+                                                                 los)
     if (L == 2) { if (rpt == 2) WL_SB(2, 2); else WL_SB(2, 1); }
     else if (L == 3) { if (rpt == 2) WL_SB(3, 2); else WL_SB(3, 1); }
     else { if (rpt == 2) WL_SB(4, 2); else WL_SB(4, 1); }

@@ -33,7 +33,12 @@ using namespace wl;
 //           equal share of the step's cell budget): the engine's sweep kernels
 //           over [pos, pos + len) -- through Bucket::cbase -- in one launch per
 //           (limb width, sweep kind) for all buckets, then k_merge* folds the
-//           chunk's split products into the resident running products;
+//           chunk's split products into the resident running products.  A
+//           bucket whose columns go past 2^32 continues above the resident
+//           table with chunks of the number line: each chunk is sieved on the
+//           device (k_sieve_big, into the bucket's own bitmap region) and swept
+//           straight from the bitmap (k_sweep_bits), as the reference's
+//           getsegprps chunks above 2^32 (cl_wilson.cpp:1368-1397);
 //   finish  requests whose buckets reached their last column: k_finish in
 //           merged mode over the request's rows, result lines and checksum
 //           (cl_wilson.cpp:872-900); the rows and slots are freed.
@@ -45,7 +50,23 @@ struct SBucket {
     bool used = false;
     uint64_t ncols = 0, cdense = 0, pos = 0;   // columns [0, ncols), dense [0, cdense), next column
     uint32_t nrows = 0, L = 2;
+    // columns above 2^32 (key >= 2^32): integers [bpos, bend) still to sieve and
+    // sweep, bend = key + 1; nroot sieving primes (67 .. sqrt(key)) for them
+    uint64_t bpos = 0, bend = 0, key = 0;
+    uint32_t nroot = 0;
+    bool done() const { return pos >= ncols && bpos >= bend; }
 };
+
+constexpr uint64_t BIG_LO = 1ull << 32;   // first integer above the resident column table
+// cost of sieving one integer above 2^32, in cells of the sweep (measured on B200)
+constexpr double BIG_SIEVE_CELLS = 1.6;
+
+uint64_t isqrt_floor(uint64_t n) {
+    uint64_t r = (uint64_t)std::sqrt((long double)n);
+    while (r * r > n) --r;
+    while ((r + 1) * (r + 1) <= n) ++r;
+    return r;
+}
 
 struct SReq {
     uint64_t id = 0, pmin = 0, pmax = 0, qcap = 0;
@@ -73,6 +94,7 @@ struct wl_server {
     uint32_t pool_cap = 0, bucket_cap = 0;
     uint64_t step_cells = 0;
     DevBuf info, mods, acc, out, pbuckets, sbuckets, bdef, ipart;
+    DevBuf bbitmap, bsegcount, boffs, bkeys, blos;   // columns above 2^32: the step's bitmaps and their keys
     std::vector<SBucket> sb;
     std::vector<Bucket> pdesc;                 // persistent descriptors (device copy: pbuckets)
     RowPool pool;                              // rows of the device row pool
@@ -170,15 +192,12 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
             if (a.byc[t].empty()) a.T[t] = Tp;
             a.byc[t].push_back(p);
         }
-        bool unsupported = false;
         for (int t = 0; t < 3; ++t) {
             if (a.byc[t].empty()) continue;
             const uint64_t key = full ? a.T[t] : std::min(a.T[t], q->qcap - 1);
-            if (key >= (1ull << 32)) unsupported = true;
             a.kt.push_back(t);
             a.keys.push_back(key);
         }
-        if (unsupported) { result[k] = WL_ERR_UNSUPPORTED; continue; }
         uint32_t r0 = 0;
         if (s->free_bids.size() < a.kt.size() || !s->pool.alloc(n, &r0)) break;
         q->r0 = r0;
@@ -188,7 +207,7 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
         for (size_t i = 0; i < a.kt.size(); ++i) {
             q->bids.push_back(*s->free_bids.begin());
             s->free_bids.erase(s->free_bids.begin());
-            need = std::max(need, a.keys[i] + 1);
+            need = std::max(need, std::min(a.keys[i], BIG_LO - 1) + 1);
         }
         result[k] = 0;
         adm.push_back(std::move(a));
@@ -198,17 +217,23 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
         for (size_t k = 0; k < nc; ++k)
             if (result[k] == 0) result[k] = e;
     };
-    // 3. column counts of every admitted bucket (all columns, dense columns)
+    // 3. column counts of every admitted bucket (all columns below 2^32, dense
+    // columns, and for buckets that go past 2^32 the sieving primes up to the
+    // square root of their key)
     std::vector<uint64_t> keys;
-    for (auto& a : adm) keys.insert(keys.end(), a.keys.begin(), a.keys.end());
-    const size_t nk = keys.size();
     for (auto& a : adm)
-        for (size_t i = 0; i < a.kt.size(); ++i) {
+        for (uint64_t key : a.keys) keys.push_back(std::min(key, BIG_LO - 1));
+    const size_t nk = keys.size();
+    size_t kj = 0;
+    for (auto& a : adm)
+        for (size_t i = 0; i < a.kt.size(); ++i, ++kj) {
             const double Td = (double)a.T[a.kt[i]];
             double qd = std::sqrt(Td) + 2;
             for (int k = 0; k < 4; ++k) qd = std::sqrt(Td * std::log(std::max(qd, 3.0))) + 2;
-            keys.push_back(std::min<uint64_t>(qd >= 1.8e19 ? ~0ull : (uint64_t)qd, a.keys[i]));
+            keys.push_back(std::min<uint64_t>(qd >= 1.8e19 ? ~0ull : (uint64_t)qd, keys[kj]));
         }
+    for (auto& a : adm)
+        for (uint64_t key : a.keys) keys.push_back(key >= BIG_LO ? isqrt_floor(key) : 0);
     int e = ensure_columns(c, need);
     if (!e) e = ensure(c->keys, keys.size() * 8);
     if (!e) e = ensure(c->counts, keys.size() * 8);
@@ -251,6 +276,11 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
             b.pos = 0;
             b.nrows = (uint32_t)a.byc[t].size();
             b.L = (uint32_t)q->L;
+            b.key = a.keys[i];
+            b.bpos = BIG_LO;
+            b.bend = b.key >= BIG_LO ? b.key + 1 : BIG_LO;
+            // column cache: cols[0 .. 17] = 2 .. 61, the presieve of k_sieve_big
+            b.nroot = b.key >= BIG_LO && cnt[2 * nk + ki] > 18 ? (uint32_t)(cnt[2 * nk + ki] - 18) : 0;
             Bucket& d = s->pdesc[bid];
             memset(&d, 0, sizeof(d));
             d.T = a.T[t];
@@ -341,66 +371,111 @@ static int serve_step(wl_server* s) {
 }
 static int serve_step_run(wl_server* s) {
     wl_ctx* c = s->c;
-    struct Work { uint32_t bid; uint64_t c0, len; bool dense; };
+    // kind 0: sparse columns of the resident table, 1: dense ones, 2: a chunk of
+    // the number line above 2^32 (integers [c0, c0 + len), sieved this step)
+    struct Work { uint32_t bid; uint64_t c0, len; int kind; };
     std::vector<Work> work;
     // the step's descriptor table covers every slot (a merge over a span of
     // rows may meet stale bucket ids of freed rows): slots without work this
     // step have nsplit = 0
     const uint32_t top = s->bucket_cap;
     size_t nact = 0;
-    for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && s->sb[bid].pos < s->sb[bid].ncols;
+    for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && !s->sb[bid].done();
     if (!nact) return 0;
     // an equal share of the cell budget per bucket; a dense column costs
-    // about five cells (prefix fold + windowed buckets)
+    // about five cells (prefix fold + windowed buckets), an integer above 2^32
+    // its share of the sieve plus a cell per prime
     const double share = (double)s->step_cells / (double)nact;
     double W = 0;
     for (uint32_t bid = 0; bid < top; ++bid) {
         SBucket& b = s->sb[bid];
-        if (!b.used || b.pos >= b.ncols) continue;
+        if (!b.used || b.done()) continue;
         Work w;
         w.bid = bid;
-        w.c0 = b.pos;
-        w.dense = b.pos < b.cdense;
-        const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
-        const uint64_t want = (uint64_t)std::max(share / per, w.dense ? 1024.0 : 8192.0);
-        const uint64_t end = w.dense ? b.cdense : b.ncols;
-        w.len = std::min<uint64_t>(end - b.pos, want);
-        // do not leave a sliver behind
-        if (end - b.pos - w.len < w.len / 4) w.len = end - b.pos;
-        W += per * (double)w.len;
+        double per, cost;
+        if (b.pos < b.ncols) {
+            w.c0 = b.pos;
+            w.kind = b.pos < b.cdense ? 1 : 0;
+            per = (double)b.nrows * (w.kind ? 5.0 : 1.0);
+            const uint64_t want = (uint64_t)std::max(share / per, w.kind ? 1024.0 : 8192.0);
+            const uint64_t end = w.kind ? b.cdense : b.ncols;
+            w.len = std::min<uint64_t>(end - b.pos, want);
+            // do not leave a sliver behind
+            if (end - b.pos - w.len < w.len / 4) w.len = end - b.pos;
+            cost = per * (double)w.len;
+        } else {
+            // whole sieve segments from bpos (a multiple of BIG_SPAN); the
+            // sieve's per-CTA offsets (CTAs x sieving primes) stay below 1 GiB
+            w.c0 = b.bpos;
+            w.kind = 2;
+            per = BIG_SIEVE_CELLS + (double)b.nrows / std::log((double)b.bpos);
+            const uint64_t rest = (b.bend - b.bpos + BIG_SPAN - 1) / BIG_SPAN;     // segments left
+            uint64_t nseg = (uint64_t)std::ceil(share / per / (double)BIG_SPAN);
+            const uint64_t max_cta = std::max<uint64_t>(1, (1ull << 28) / std::max<uint32_t>(b.nroot, 1));
+            nseg = std::max<uint64_t>(1, std::min<uint64_t>(nseg, 8 * max_cta));
+            if (rest - std::min(rest, nseg) < nseg / 4) nseg = rest;
+            nseg = std::min(nseg, rest);
+            w.len = nseg * BIG_SPAN;
+            cost = per * (double)w.len;
+        }
+        W += cost;
         work.push_back(w);
     }
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
     std::vector<Bucket> sbk(top);
     memset(sbk.data(), 0, sbk.size() * sizeof(Bucket));
-    struct Grp { int L, rpt; bool dense; std::vector<SweepItem> items; };
+    struct Grp { int L, rpt, kind; std::vector<SweepItem> items; };
     std::vector<Grp> groups;
-    uint64_t part_total = 0;
+    uint64_t part_total = 0, bwords = 0, boffs_need = 0, bseg_need = 0;
     uint32_t def_total = 0;
     std::vector<uint32_t> bucket_splits(top, 0);
+    std::vector<uint64_t> bkeys, blos;
     for (const Work& w : work) {
         const SBucket& b = s->sb[w.bid];
         Bucket& x = sbk[w.bid];
         x = s->pdesc[w.bid];
-        x.cbase = (uint32_t)w.c0;
-        x.ncols = (uint32_t)w.len;
         int rpt = 1;
         uint32_t tps = 256;
-        if (w.dense) {
-            dense_shape(b.nrows, &rpt, &tps);
-        } else {
-            rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows);
+        uint64_t S;
+        if (w.kind == 2) {
+            // the chunk's bitmap region: its words from bwords on
+            const uint64_t nseg = w.len / BIG_SPAN, nw = nseg * BIG_WORDS;
+            if (bwords + nw >= (1ull << 32)) return WL_ERR_UNSUPPORTED;
+            if (bkeys.empty()) { bkeys.assign(top, 0); blos.assign(top, 0); }
+            bkeys[w.bid] = b.key;
+            blos[w.bid] = w.c0;
+            x.cbase = (uint32_t)bwords;
+            x.ncols = (uint32_t)nw;
+            bwords += nw;
+            const uint64_t ncta = (nseg + 7) / 8;
+            boffs_need = std::max(boffs_need, ncta * std::max<uint32_t>(b.nroot, 1));
+            bseg_need = std::max(bseg_need, nseg);
+            if (b.nrows >= 512) rpt = 2;
             if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
+            // splits by the sweep's cells per row: the chunk's primes, about len / ln(c0)
+            S = (uint64_t)std::ceil((double)rpt * ((double)w.len / std::log((double)w.c0)) * target_threads / W);
+            S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, nw / 256)));
+            x.cdense = 0;
+            x.ndense = 0;
+        } else {
+            const bool dense = w.kind == 1;
+            x.cbase = (uint32_t)w.c0;
+            x.ncols = (uint32_t)w.len;
+            if (dense) {
+                dense_shape(b.nrows, &rpt, &tps);
+            } else {
+                rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows);
+                if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
+            }
+            const double per = (double)b.nrows * (dense ? 5.0 : 1.0);
+            S = (uint64_t)std::ceil((double)rpt * per / (double)b.nrows * (double)w.len * target_threads / W);
+            const uint64_t minlen = dense ? 256 : 2048;
+            S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, w.len / minlen)));
+            if (dense) S = std::max<uint64_t>(S, std::min<uint64_t>((w.len + 1023) / 1024, w.len / 256 ? w.len / 256 : 1));
+            x.cdense = dense ? (uint32_t)w.len : 0;
+            x.ndense = dense ? (uint32_t)S : 0;
         }
-        const double per = (double)b.nrows * (w.dense ? 5.0 : 1.0);
-        uint64_t S = (uint64_t)std::ceil((double)rpt * per / (double)b.nrows * (double)w.len *
-                                         target_threads / W);
-        const uint64_t minlen = w.dense ? 256 : 2048;
-        S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, w.len / minlen)));
-        if (w.dense) S = std::max<uint64_t>(S, std::min<uint64_t>((w.len + 1023) / 1024, w.len / 256 ? w.len / 256 : 1));
         x.nsplit = (uint32_t)S;
-        x.cdense = w.dense ? (uint32_t)w.len : 0;
-        x.ndense = w.dense ? (uint32_t)S : 0;
         x.dstart = 0;
         x.part_base = part_total;
         x.def_base = def_total;
@@ -409,9 +484,9 @@ static int serve_step_run(wl_server* s) {
         bucket_splits[w.bid] = (uint32_t)S;
         Grp* g = nullptr;
         for (auto& gg : groups)
-            if (gg.L == (int)b.L && gg.rpt == rpt && gg.dense == w.dense) g = &gg;
+            if (gg.L == (int)b.L && gg.rpt == rpt && gg.kind == w.kind) g = &gg;
         if (!g) {
-            groups.push_back({ (int)b.L, rpt, w.dense, {} });
+            groups.push_back({ (int)b.L, rpt, w.kind, {} });
             g = &groups.back();
         }
         if (tps == 256) {
@@ -429,12 +504,40 @@ static int serve_step_run(wl_server* s) {
     RC(ensure(c->items, all.size() * sizeof(SweepItem) + 16));
     RC(ensure(c->part, part_total * 16 + 16));
     RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
+    if (bwords) {
+        RC(ensure(s->bbitmap, bwords * 4));
+        RC(ensure(s->bsegcount, bseg_need * 4 + 16));
+        RC(ensure(s->boffs, boffs_need * 4 + 16));
+        RC(ensure(s->bkeys, (size_t)top * 8));
+        RC(ensure(s->blos, (size_t)top * 8));
+    }
     cudaEventRecord(s->e0, c->st);
     CK(cudaMemcpyAsync(s->sbuckets.p, sbk.data(), sbk.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->items.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, c->st));
+    if (bwords) {
+        CK(cudaMemcpyAsync(s->bkeys.p, bkeys.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(s->blos.p, blos.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
+        // sieve every chunk above 2^32 into its bitmap region (the sieving
+        // primes 67 .. sqrt(key) come from the resident column table; one
+        // launch after another on the stream, so they share the offsets)
+        for (const Work& w : work) {
+            if (w.kind != 2) continue;
+            const SBucket& b = s->sb[w.bid];
+            const uint32_t nseg = (uint32_t)(w.len / BIG_SPAN);
+            launch_sieve_big(w.c0, std::min(w.c0 + w.len, b.bend), nseg, 8, as<uint32_t>(c->cols) + 18, b.nroot,
+                             as<uint32_t>(s->boffs), as<uint32_t>(s->bbitmap) + sbk[w.bid].cbase,
+                             as<uint32_t>(s->bsegcount), c->st);
+            s->ws.launches++;
+        }
+    }
     size_t ioff = 0;
     for (auto& g : groups) {
-        if (g.dense)
+        if (g.kind == 2)
+            launch_sweep_bits(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
+                              as<SweepItem>(c->items) + ioff, as<RowMod>(s->mods), as<uint32_t>(s->bbitmap), 0,
+                              as<uint64_t>(s->bkeys), as<uint4>(c->part), as<Deficit>(c->defs), c->st,
+                              as<uint64_t>(s->blos));
+        else if (g.kind == 1)
             launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
                                as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(c->part),
                                as<Deficit>(c->defs), c->st,
@@ -478,7 +581,11 @@ static int serve_step_run(wl_server* s) {
     cudaEventElapsedTime(&ms, s->e0, s->e1);
     s->ws.ms_steps += ms;
     s->ws.steps++;
-    for (const Work& w : work) s->sb[w.bid].pos += w.len;
+    for (const Work& w : work) {
+        SBucket& b = s->sb[w.bid];
+        if (w.kind == 2) b.bpos = std::min(w.c0 + w.len, b.bend);
+        else b.pos += w.len;
+    }
     return 0;
 }
 
@@ -596,7 +703,7 @@ static void serve_loop(wl_server* s) {
         std::vector<SReq*> keep;
         for (SReq* q : s->active) {
             bool done = true;
-            for (uint32_t bid : q->bids) done &= s->sb[bid].pos >= s->sb[bid].ncols;
+            for (uint32_t bid : q->bids) done &= s->sb[bid].done();
             bool cancel;
             {
                 std::lock_guard<std::mutex> lk(s->mu);
@@ -662,7 +769,6 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
 int wl_server_submit(wl_server* s, uint64_t pmin, uint64_t pmax, uint64_t q_cap, uint64_t* id) {
     if (!s) return WL_ERR_ARG;
     RC(wl_check_range(pmin, pmax));
-    if (q_cap > (1ull << 32)) return WL_ERR_UNSUPPORTED;
     SReq* q = new SReq();
     q->pmin = pmin;
     q->pmax = pmax;
@@ -780,7 +886,8 @@ void wl_server_close(wl_server* s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->c->device);
     cudaStreamSynchronize(s->c->st);
-    DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->sbuckets, &s->bdef, &s->ipart };
+    DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->sbuckets, &s->bdef, &s->ipart,
+                       &s->bbitmap, &s->bsegcount, &s->boffs, &s->bkeys, &s->blos };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);

@@ -271,10 +271,10 @@ int wl_autotune(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap, u
  * that arrive while others run share the GPU with them.  Each request's
  * results are bit-identical to wl_search / wl_rows on the same range.
  *
- * Limits: the columns of a request stay below 2^32 (q_cap <= 2^32, or a full
- * search whose class targets are below 2^32: p below about 8.5e9);
- * otherwise the request fails with WL_ERR_UNSUPPORTED.  A request larger than
- * the whole pool fails with WL_ERR_NOMEM.  All functions are thread-safe. */
+ * Columns above 2^32 (full searches with p above about 8.5e9, or q_cap above
+ * 2^32) are sieved in chunks of the number line inside the step loop, each
+ * chunk sized to the bucket's share of the step.  A request larger than the
+ * whole pool fails with WL_ERR_NOMEM.  All functions are thread-safe. */
 typedef struct wl_server wl_server;
 
 typedef struct {

@@ -89,18 +89,80 @@ def test_cancel_and_errors(expected):
         srv.cancel(big)
         assert srv.wait(big, 600_000).state == "cancelled"
         _check(srv, small, CAPPED[0], expected)
-        # full search with class targets above 2^32: not served
-        bad = srv.submit(10**13, 10**13 + 1000)
-        info = srv.wait(bad, 600_000)
-        assert info.state == "failed" and info.rc == -4
         # no primes in [24, 29)
         none = srv.submit(24, 29)
         info = srv.wait(none, 600_000)
         assert info.state == "failed" and info.rc == -3
         with pytest.raises(wl.WilsonError):
-            srv.submit(10**9, 10**9 + 100, (1 << 32) + 1)
-        with pytest.raises(wl.WilsonError):
             srv.submit(4, 100)
         # the server keeps serving after failures
         rid = srv.submit(*CAPPED[3])
         _check(srv, rid, CAPPED[3], expected)
+
+
+def test_columns_above_2_32(engine, golden):
+    # self-test cases 1 and 2 (class targets 2.07e11 and 2.77e11, cl_wilson.cpp:2007-2030):
+    # their columns above 2^32 are sieved in chunks inside the step loop.  Alone,
+    # then together with small requests that keep arriving; and a capped request
+    # whose cap lies above 2^32.
+    kats = golden["kat"][:2]
+    small = [(lo, hi, 0) for lo, hi in FULL[:2]] + [CAPPED[2], CAPPED[3]]
+    want_small = {}
+    for lo, hi, q in small:
+        rows, _ = engine.rows(lo, hi, q_cap=q)
+        want_small[(lo, hi, q)] = rows
+    cap = (1 << 32) + (1 << 26)
+    capped_rows, _ = engine.rows(10**13, 10**13 + 2000, q_cap=cap)
+
+    def check_kat(srv, rid, k):
+        info = srv.wait(rid, 600_000)
+        assert info.state == "done", info
+        assert "%016X" % info.checksum == k["checksum"]
+        assert srv.results(rid) == [(k["last_prime"], k["last_value"])]
+
+    def check_small(srv, rid, key):
+        info = srv.wait(rid, 600_000)
+        assert info.state == "done", (key, info)
+        got = srv.rows(rid)
+        for f in ("p", "s0", "s1", "rem", "quot"):
+            assert np.array_equal(got[f], want_small[key][f]), (key, f)
+        return info.ms_latency
+
+    with wl.Server(0) as srv:
+        for k in kats:
+            check_kat(srv, srv.submit(k["pmin"], k["pmax"]), k)
+        rid = srv.submit(10**13, 10**13 + 2000, cap)
+        assert srv.wait(rid, 600_000).state == "done"
+        got = srv.rows(rid)
+        assert np.array_equal(got["s0"], capped_rows["s0"]) and np.array_equal(got["s1"], capped_rows["s1"])
+        alone = [check_small(srv, srv.submit(*key), key) for key in small]
+        # mixed: both long requests, then small ones submitted while they run
+        big = [srv.submit(k["pmin"], k["pmax"]) for k in kats]
+        mixed = []
+        for _ in range(3):
+            ids = [(srv.submit(*key), key) for key in small]
+            mixed += [check_small(srv, rid, key) for rid, key in ids]
+        for rid, k in zip(big, kats):
+            check_kat(srv, rid, k)
+        st = srv.stats()
+        assert st["failed"] == 0 and st["peak_active"] > 1
+    assert len(alone) == len(small) and len(mixed) == 3 * len(small)
+
+
+@pytest.mark.parametrize("lo,hi,q", [(10**6, 10**6 + 5000, 0), (10**13, 10**13 + 4000, 1 << 20),
+                                     ((1 << 62) - 8000, (1 << 62) - 1, 1 << 20)])
+def test_one_request_per_limb_width_against_oracle(lo, hi, q):
+    # 2-, 3- and 4-limb rows served alone, checked against the oracle directly
+    import oracle
+    with wl.Server(0) as srv:
+        rid = srv.submit(lo, hi, q)
+        info = srv.wait(rid, 600_000)
+        assert info.state == "done", info
+        got = srv.rows(rid)
+    sel = list(range(0, len(got), max(1, len(got) // 16)))
+    want, _ = oracle.search(lo, hi, qcap=q, rows=sel)
+    assert np.array_equal(got["p"], want["p"])
+    fields = ("s0", "s1") if q else ("s0", "s1", "rem", "quot")
+    for i in sel:
+        for f in fields:
+            assert int(got[f][i]) == int(want[f][i]), (lo, f, int(got["p"][i]))

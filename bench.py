@@ -319,7 +319,8 @@ def run_reference(args, rank, world):
     return 0
 
 
-def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, warmup, tuning=None):
+def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, warmup, tuning=None,
+                   shares="least-work"):
     """The serving stream through a serving session: every request submitted
     at its arrival time, all waited for.  Returns the record (throughput over
     the device-busy time, e2e over the stream's wall time, latencies)."""
@@ -327,15 +328,22 @@ def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, w
     import clwilson_b200 as wl
     reqs = serving_requests(1, requests, rate, max_width)[rank::world]
     L = max(limbs_for(b - 1) for _, a, b in reqs)
-    srv = wl.Server(local, tuning=tuning)
+    srv = wl.Server(local, tuning=tuning, shares=shares)
+
+    late = []
 
     def stream(reqs):
+        # submit each request at its arrival time; `late` records how far behind
+        # its schedule each submission was (a stalled host thread shows up there
+        # as a burst of submissions, not as server latency)
         ids = []
+        del late[:]
         t0 = time.perf_counter()
         for t, a, b in reqs:
             dt = t - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
+            late.append(1e3 * max(0.0, time.perf_counter() - t0 - t))
             ids.append(srv.submit(a, b, q_cap))
         infos = [srv.wait(i, 3600e3) for i in ids]
         t1 = time.perf_counter()
@@ -369,14 +377,15 @@ def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, w
     lat = np.array(lat)
     (wall, busy_s), (cells, rows, nreq, nbad) = merge_over_ranks(dist, [wall, busy_s],
                                                                  [cells, rows, len(reqs), len(bad)])
-    host_us = 1e3 * (d["ms_wall_steps"] - d["ms_steps"]) / max(1, d["steps"])
+    # host time planning and queueing a step; it overlaps the previous step on the GPU
+    plan_us = 1e3 * d["ms_wall_steps"] / max(1, d["steps"])
     return {
         "metric": "128-bit mulmods/s (capped column sweep, serving)", "value": cells / busy_s,
         "unit": "mulmods/s", "higher_is_better": True, "n_gpus": world, "steps": 1, "warmup": warmup,
         "ms_per_step": 1e3 * wall,
         "config": {"workload": f"serving: {int(nreq)} requests from default_rng(1), Poisson at {rate}/s, "
                                f"widths truncated to {max_width}, columns q < {q_cap}",
-                   "rate_per_s": rate, "requests": int(nreq), "q_cap": q_cap, "limbs_max": L,
+                   "rate_per_s": rate, "requests": int(nreq), "q_cap": q_cap, "limbs_max": L, "shares": shares,
                    "test_primes": rows, "column_mulmods": cells,
                    "parallelism": f"requests sharded round-robin, dp{world}"},
         "e2e": {"value": cells / wall, "unit": "mulmods/s", "primes_per_s": rows / wall,
@@ -384,13 +393,15 @@ def serving_record(local, rank, world, dist, requests, rate, max_width, q_cap, w
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max()), "mean": float(lat.mean()), "requests": int(lat.size)},
         "queue_ms_p50": float(np.percentile(queued, 50)),
+        "submit_late_ms": {"p99": float(np.percentile(late, 99)), "max": float(max(late))},
         "failed": int(nbad),
         "server": {"steps": d["steps"], "admitted": d["admitted"], "completed": d["completed"],
                    "launches": d["launches"], "peak_active": st1["peak_active"], "busy_s": busy_s,
-                   "host_us_per_step": host_us,
+                   "plan_us_per_step": plan_us,
                    "device_us_per_step": 1e3 * d["ms_steps"] / max(1, d["steps"]),
-                   "wall_s": {"steps": d["ms_wall_steps"] / 1e3, "admit": d["ms_wall_admit"] / 1e3,
-                              "finish": d["ms_wall_finish"] / 1e3}},
+                   "scheduler_wall_s": {"plan_and_queue": d["ms_wall_steps"] / 1e3,
+                                        "admit": d["ms_wall_admit"] / 1e3,
+                                        "wait_and_complete": d["ms_wall_finish"] / 1e3}},
         "gpu_launches": d["launches"],
         "clocks": clk.summary(),
     }
@@ -418,7 +429,7 @@ def run_serving(args, rank, world, local):
         tuning = eng.autotune([(a, b) for _, a, b in reqs[:64]], q_cap)
         eng.close()
     line = serving_record(local, rank, world, dist, args.requests, args.rate, args.max_width, q_cap,
-                          max(3, args.warmup), tuning)
+                          max(3, args.warmup), tuning, args.serving_shares)
     line.update({"scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
                  "tuning": tuning if tuning is not None else "defaults",
                  "roofline": {"bound": "imad", "peak": peak_mad / 1e12, "unit": "TOP/s", "achieved": None,
@@ -647,6 +658,8 @@ def main():
     ap.add_argument("--serving-autotune", action="store_true",
                     help="serving: tune the kernels on the first 64 requests run as one batch (batch throughput; "
                          "the default kernels are kept otherwise)")
+    ap.add_argument("--serving-shares", default="least-work", choices=["least-work", "equal"],
+                    help="serving: how a scheduler step's budget is split between requests")
     ap.add_argument("--no-sub-records", action="store_true",
                     help="plain-small: skip the batched and serving records that the default run adds")
     ap.add_argument("--sub-batched-width", type=int, default=20000,
@@ -690,7 +703,8 @@ def main():
     tuning = None if args.no_autotune else eng.autotune(tune_ranges, q_cap)
     t_tune = time.perf_counter() - t_tune
     peak_mad = wl.probe("mad", local)
-    peak_cell = wl.probe("cell%d" % L, local)
+    # the register-only rate of the cell formulation the sweeps run (wide products)
+    peak_cell = wl.probe("cell%dw" % L, local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MiB > L2
 
     def step():
@@ -769,6 +783,8 @@ def main():
                      "ops_per_cell": OPS_PER_CELL[L],
                      "cells_executed_per_step": exec_cells / args.steps,
                      "dense_share_of_cells": dense_cells / max(1.0, exec_cells),
+                     "dense_per_step": {k: sum(getattr(s, "dense_" + k) for s in stats) / args.steps
+                                        for k in ("column_cells", "window_cells", "products")},
                      "cell_peak_per_s": peak_cell, "cell_frac": (exec_cells / sweep_s) / peak_cell,
                      "peak_source": "wl_probe mad.lo.u32 microbenchmark, this GPU, this run",
                      "count": "cells executed: one per (row, column), plus the dense sweep's window cells and "
@@ -847,10 +863,10 @@ def main():
         line["parity_sample_ok"] = line["parity_sample"]["ok"]
     if args.workload == "plain-small" and not args.no_sub_records:
         # the rest of the headline metric: batched against plain, and serving latency
-        line["batched"] = batched_record(eng, rank, world, dist, stream, flush, args.sub_batched_width,
-                                         args.sub_batched_steps, 1)
         line["serving"] = serving_record(local, rank, world, dist, args.sub_serving_requests,
                                          args.sub_serving_rate, 2000, 2**28, 3)
+        line["batched"] = batched_record(eng, rank, world, dist, stream, flush, args.sub_batched_width,
+                                         args.sub_batched_steps, 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -96,7 +96,7 @@ class _Tuning(ctypes.Structure):
 
 
 class _ServerOpts(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int), ("pad", ctypes.c_uint32), ("pool_bytes", ctypes.c_uint64),
+    _fields_ = [("device", ctypes.c_int), ("shares", ctypes.c_uint32), ("pool_bytes", ctypes.c_uint64),
                 ("step_cells", ctypes.c_uint64), ("tuning", ctypes.c_void_p)]
 
 
@@ -130,7 +130,9 @@ SYMBOLS = ("wl_open", "wl_close", "wl_strerror", "wl_stream", "wl_check_range", 
            "wl_column_product_noalloc", "wl_get_tuning", "wl_set_tuning", "wl_autotune",
            "wl_server_open", "wl_server_submit", "wl_server_poll", "wl_server_wait", "wl_server_results",
            "wl_server_rows", "wl_server_cancel", "wl_server_release", "wl_server_stats_get", "wl_server_close")
-PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5}
+# cellL: the carry-chain cell; cellLw: the wide-product cell the sweeps run by default
+PROBES = {"mad": 0, "madhi": 1, "cell2": 2, "cell3": 3, "cell4": 4, "madwide": 5,
+          "cell2w": 101, "cell3w": 111, "cell4w": 121}
 
 _lib = None
 
@@ -484,11 +486,13 @@ class Server:
     column sweeps with the requests already running; each request's results
     equal those of ``Engine.search`` / ``Engine.rows`` on its range."""
 
-    def __init__(self, device: int = 0, pool_bytes: int = 0, step_cells: int = 0, tuning: Optional[dict] = None):
+    def __init__(self, device: int = 0, pool_bytes: int = 0, step_cells: int = 0, tuning: Optional[dict] = None,
+                 shares: str = "least-work"):
         self._L = load_library()
         self._srv = ctypes.c_void_p()
         self._tune = _Tuning.from_dict(tuning) if tuning else None
-        o = _ServerOpts(device, 0, pool_bytes, step_cells,
+        policy = {"least-work": 0, "equal": 1}[shares]
+        o = _ServerOpts(device, policy, pool_bytes, step_cells,
                         ctypes.cast(ctypes.pointer(self._tune), ctypes.c_void_p) if tuning else None)
         rc = self._L.wl_server_open(ctypes.byref(o), ctypes.byref(self._srv))
         if rc:

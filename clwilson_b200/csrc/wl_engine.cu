@@ -61,7 +61,7 @@ static void default_tuning(wl_ctx* c) {
     for (int L = 2; L <= 4; ++L) {
         int k = kernel;
         if (!sort) k = (cfg == 42 || (cfg == 0 && L != 4)) ? DENSE_SWITCH_W4 : DENSE_SWITCH_W3;
-        if (forced >= 0 && forced <= DENSE_SMEM_W4) k = forced;
+        if (forced >= 0 && forced <= DENSE_SORTED_W3_2CTA) k = forced;
         c->tune.sparse_variant[L - 2] = c->cell_variant;
         c->tune.sparse_rpt[L - 2] = 2;
         c->tune.dense_kernel[L - 2] = k;
@@ -246,25 +246,22 @@ static int run_big_columns(wl_ctx* c, const std::vector<Bucket>& db, const std::
             x.part_base = part_total;
             x.def_base = def_total;
             if (!nw[b]) { x.nsplit = 0; continue; }
-            int rpt, tps;
-            if (x.nrows >= 512) { rpt = 2; tps = 256; }
-            else if (x.nrows >= 256) { rpt = 1; tps = 256; }
-            else { rpt = 1; tps = 1; while (tps < (int)x.nrows) tps <<= 1; }
+            const int rpt = x.nrows >= 512 ? 2 : 1;
             uint64_t S = (uint64_t)std::ceil((double)rpt * (double)nw[b] * target_threads / W);
             S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, nw[b] / 256)));
             x.nsplit = (uint32_t)S;
             maxs = std::max<uint32_t>(maxs, x.nsplit);
             part_total += S * x.nrows;
             def_total += (uint32_t)S;
-            Grp* g = nullptr;
-            for (auto& gg : groups) if (gg.L == (int)x.L && gg.rpt == rpt) g = &gg;
-            if (!g) { groups.push_back({ (int)x.L, rpt, {} }); g = &groups.back(); }
-            if (tps == 256) {
-                for (uint32_t r0 = 0; r0 < x.nrows; r0 += 256 * rpt)
-                    for (uint32_t s2 = 0; s2 < S; ++s2) g->items.push_back({ (uint32_t)b, r0, s2, 256u });
-            } else {
-                const uint32_t per = 256 / tps;
-                for (uint32_t s2 = 0; s2 < S; s2 += per) g->items.push_back({ (uint32_t)b, 0, s2, (uint32_t)tps });
+            std::vector<RowTile> tiles;
+            row_tiles(x.nrows, rpt, 1, tiles);
+            for (const RowTile& t : tiles) {
+                Grp* g = nullptr;
+                for (auto& gg : groups) if (gg.L == (int)x.L && gg.rpt == t.rpt) g = &gg;
+                if (!g) { groups.push_back({ (int)x.L, t.rpt, {} }); g = &groups.back(); }
+                tile_items(t, 0, (uint32_t)S, [&](uint32_t r0, uint32_t s2, uint32_t tp) {
+                    g->items.push_back({ (uint32_t)b, r0, s2, tp });
+                });
             }
         }
         // the previous window's copies must be done before these host vectors change
@@ -570,10 +567,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         b.L = h.L;
         b.type = h.type;
         b.range = h.range;
-        int rpt, tps;
-        if (b.nrows >= 512) { rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows); tps = 256; }
-        else if (b.nrows >= 256) { rpt = 1; tps = 256; }
-        else { rpt = 1; tps = 1; while (tps < (int)b.nrows) tps <<= 1; }
+        const int rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows);
         const uint64_t nd = ndn[i];
         uint64_t Sd = 0, Ss = 0;
         plan_splits(i, scale, &Sd, &Ss);
@@ -597,28 +591,24 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         part_total += S * b.nrows;
         def_total += (uint32_t)S;
         out.cells += (uint64_t)b.nrows * b.ncols;
+        std::vector<RowTile> tiles;
         if (Ss) {
-            auto& items = group_for((int)b.L, rpt, false);
-            if (tps == 256) {
-                const uint32_t tile = 256 * rpt;
-                for (uint32_t r0 = 0; r0 < b.nrows; r0 += tile)
-                    for (uint32_t s2 = (uint32_t)Sd; s2 < S; ++s2) items.push_back({ oi, r0, s2, 256u });
-            } else {
-                const uint32_t per = 256 / tps;
-                for (uint32_t s2 = (uint32_t)Sd; s2 < S; s2 += per) items.push_back({ oi, 0, s2, (uint32_t)tps });
+            row_tiles(b.nrows, rpt, 1, tiles);
+            for (const RowTile& t : tiles) {
+                auto& items = group_for((int)b.L, t.rpt, false);
+                tile_items(t, (uint32_t)Sd, (uint32_t)S,
+                           [&](uint32_t r0, uint32_t s2, uint32_t tp) { items.push_back({ oi, r0, s2, tp }); });
             }
         }
         if (Sd) {
             int drpt;
             uint32_t dtps;
             dense_shape(b.nrows, &drpt, &dtps);
-            auto& items = group_for((int)b.L, drpt, true);
-            if (dtps == 256) {
-                for (uint32_t r0 = 0; r0 < b.nrows; r0 += 256 * drpt)
-                    for (uint32_t s2 = 0; s2 < Sd; ++s2) items.push_back({ oi, r0, s2, 256u });
-            } else {
-                const uint32_t per = 256 / dtps;
-                for (uint32_t s2 = 0; s2 < Sd; s2 += per) items.push_back({ oi, 0, s2, dtps });
+            row_tiles(b.nrows, drpt, 8, tiles, true);
+            for (const RowTile& t : tiles) {
+                auto& items = group_for((int)b.L, t.rpt, true);
+                tile_items(t, 0, (uint32_t)Sd,
+                           [&](uint32_t r0, uint32_t s2, uint32_t tp) { items.push_back({ oi, r0, s2, tp }); });
             }
         }
         for (uint32_t k = 0; k < b.nrows; ++k) {
@@ -1142,7 +1132,8 @@ int wl_set_tuning(wl_ctx* c, const wl_tuning* t) {
     for (int i = 0; i < 3; ++i) {
         if (t->sparse_variant[i] < 0 || t->sparse_variant[i] > 3 ||
             (t->sparse_rpt[i] != 1 && t->sparse_rpt[i] != 2 && t->sparse_rpt[i] != 4) ||
-            t->dense_kernel[i] < 0 || t->dense_kernel[i] > 5 || t->dense_hstep[i] < 1 || t->dense_hstep[i] > 4096)
+            t->dense_kernel[i] < 0 || t->dense_kernel[i] > DENSE_SORTED_W3_2CTA || t->dense_hstep[i] < 1 ||
+            t->dense_hstep[i] > 4096)
             return WL_ERR_ARG;
     }
     if (t->merge_cta_min < 1) return WL_ERR_ARG;
@@ -1206,9 +1197,9 @@ static int tune_on(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, uint3
         bool b;
         RC(trial(t, &b));
     }
-    const int dense_c[7][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 16 }, { DENSE_SORTED_W4, 8 },
-                                { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 }, { DENSE_SMEM_W3, 8 },
-                                { DENSE_SMEM_W4, 8 } };
+    const int dense_c[9][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 12 }, { DENSE_SORTED_W3, 16 },
+                                { DENSE_SORTED_W4, 8 }, { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 },
+                                { DENSE_SMEM_W3, 8 }, { DENSE_SMEM_W4, 8 }, { DENSE_SORTED_W3_2CTA, 8 } };
     for (auto& dc : dense_c) {
         wl_tuning t = c->tune;
         apply([&](int i) { t.dense_kernel[i] = dc[0]; t.dense_hstep[i] = dc[1]; });

@@ -135,10 +135,11 @@ void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaSt
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                   const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
 // dense sweep kernels: digit-sorted windows (3-bit at 3 CTAs/SM, 4-bit at
-// 2 CTAs/SM), a per-column bucket switch (same two shapes), or digit-sorted
-// windows with the buckets in shared memory (3-bit at 4 CTAs/SM, 4-bit at 2)
+// 2 CTAs/SM, 3-bit at 2 CTAs/SM with every value in registers), a per-column
+// bucket switch (3- and 4-bit), or digit-sorted windows with the buckets in
+// shared memory (3-bit at 4 CTAs/SM, 4-bit at 2)
 enum { DENSE_SORTED_W3 = 0, DENSE_SORTED_W4 = 1, DENSE_SWITCH_W3 = 2, DENSE_SWITCH_W4 = 3, DENSE_SMEM_W3 = 4,
-       DENSE_SMEM_W4 = 5 };
+       DENSE_SMEM_W4 = 5, DENSE_SORTED_W3_2CTA = 6 };
 // work (may be null): adds the launch's column cells, window cells and full products, summed over rows
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,

@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(256)
 k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
         const uint32_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
     const SweepItem it = items[blockIdx.x];
+    if (threadIdx.x >= (256 / it.tps) * it.tps) return;   // lanes past the CTA's last whole group
     const Bucket bk = buckets[it.bucket];
     const uint32_t s = it.split0 + threadIdx.x / it.tps;
     if (s >= bk.nsplit) return;
@@ -527,7 +528,10 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     const uint32_t g = threadIdx.x / tps, lt = threadIdx.x % tps;
     const uint32_t KG = DENSE_CHUNK / G;          // staged columns per split and chunk
     const uint32_t s = it.split0 + g;
-    const bool has_split = s < bk.ndense;
+    // lanes past the CTA's last whole group (tps need not divide 256) take no
+    // split; they still pass every barrier, and g == G < DENSE_GMAX keeps
+    // their per-group table rows in bounds
+    const bool has_split = g < G && s < bk.ndense;
     const uint64_t T = bk.T;
 
     uint32_t n[RPT][L];
@@ -1356,6 +1360,7 @@ __global__ void __launch_bounds__(256)
 k_sweep64(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
           const uint64_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
     const SweepItem it = items[blockIdx.x];
+    if (threadIdx.x >= (256 / it.tps) * it.tps) return;   // lanes past the CTA's last whole group
     const Bucket bk = buckets[it.bucket];
     const uint32_t s = it.split0 + threadIdx.x / it.tps;
     if (s >= bk.nsplit) return;
@@ -1455,6 +1460,7 @@ k_sweep_bits(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ i
              const uint32_t* __restrict__ bitmap, uint64_t lo, const uint64_t* __restrict__ keys,
              uint4* __restrict__ part, Deficit* __restrict__ defs, const uint64_t* __restrict__ los) {
     const SweepItem it = items[blockIdx.x];
+    if (threadIdx.x >= (256 / it.tps) * it.tps) return;   // lanes past the CTA's last whole group
     const Bucket bk = buckets[it.bucket];
     const uint32_t s = it.split0 + threadIdx.x / it.tps;
     if (s >= bk.nsplit) return;
@@ -1833,6 +1839,8 @@ void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, 
         if (L == 2) WL_D(2, 3, 3, 1, 0); else if (L == 3) WL_D(3, 3, 3, 1, 0); else WL_D(4, 3, 3, 1, 0);
     } else if (kernel == DENSE_SWITCH_W4) {
         if (L == 2) WL_D(2, 2, 4, 1, 0); else if (L == 3) WL_D(3, 2, 4, 1, 0); else WL_D(4, 2, 4, 1, 0);
+    } else if (kernel == DENSE_SORTED_W3_2CTA) {
+        if (L == 2) WL_D(2, 2, 3, 1, 1); else if (L == 3) WL_D(3, 2, 3, 1, 1); else WL_D(4, 2, 3, 1, 1);
     } else {   // DENSE_SORTED_W3
         if (L == 2) WL_D(2, 3, 3, 1, 1); else if (L == 3) WL_D(3, 3, 3, 1, 1); else WL_D(4, 3, 3, 1, 1);
     }

@@ -29,8 +29,8 @@ using namespace wl;
 //           primes, classes and targets, column counts, moduli, and for a full
 //           search the consecutive-integer tail folded into each row's running
 //           product (k_iterate + k_tail_merge);
-//   step    every admitted bucket advances by one chunk of its columns (an
-//           equal share of the step's cell budget): the engine's sweep kernels
+//   step    every admitted bucket advances by one chunk of its columns (its
+//           share of the step's cell budget): the engine's sweep kernels
 //           over [pos, pos + len) -- through Bucket::cbase -- in one launch per
 //           (limb width, sweep kind) for all buckets, then k_merge* folds the
 //           chunk's split products into the resident running products.  A
@@ -40,8 +40,14 @@ using namespace wl;
 //           straight from the bitmap (k_sweep_bits), as the reference's
 //           getsegprps chunks above 2^32 (cl_wilson.cpp:1368-1397);
 //   finish  requests whose buckets reached their last column: k_finish in
-//           merged mode over the request's rows, result lines and checksum
+//           merged mode over the request's rows, queued right behind the step,
+//           then the rows read back, result lines and checksum
 //           (cl_wilson.cpp:872-900); the rows and slots are freed.
+// Steps are pipelined: two sets of step buffers, so the scheduler plans and
+// queues step k+1 while step k runs, and completes step k (its timing and the
+// requests whose lift followed it) meanwhile.  Admissions and cancellations
+// drain the pipeline first (admission synchronises the stream and may grow
+// the column table; a cancelled request's rows must not be in use).
 // ===========================================================================
 
 namespace {
@@ -54,7 +60,9 @@ struct SBucket {
     // sweep, bend = key + 1; nroot sieving primes (67 .. sqrt(key)) for them
     uint64_t bpos = 0, bend = 0, key = 0;
     uint32_t nroot = 0;
+    bool stop = false;                         // cancelled: no further chunks
     bool done() const { return pos >= ncols && bpos >= bend; }
+    bool idle() const { return stop || done(); }
 };
 
 constexpr uint64_t BIG_LO = 1ull << 32;   // first integer above the resident column table
@@ -84,6 +92,8 @@ struct SReq {
     uint64_t tested = 0;              // set under the server's mutex
     std::vector<wl_row> rows;         // ascending p, once done
     std::vector<wl_result> lines;
+    bool finishing = false;           // its lift is queued behind a step (scheduler thread only)
+    bool cancel_seen = false;         // the scheduler stopped its buckets (scheduler thread only)
     double t_submit = 0, t_admit = 0, t_done = 0;
 };
 
@@ -93,8 +103,20 @@ struct wl_server {
     wl_ctx* c = nullptr;
     uint32_t pool_cap = 0, bucket_cap = 0;
     uint64_t step_cells = 0;
-    DevBuf info, mods, acc, out, pbuckets, sbuckets, bdef, ipart;
-    DevBuf bbitmap, bsegcount, boffs, bkeys, blos;   // columns above 2^32: the step's bitmaps and their keys
+    uint32_t shares = WL_SHARES_LEAST_WORK;
+    DevBuf info, mods, acc, out, pbuckets, bdef, ipart;
+    // Two sets of a step's buffers: the scheduler plans and queues step k+1
+    // into one set while step k still runs on the other, and completes step k
+    // (its timing, the requests whose lift followed it) meanwhile.
+    struct Slot {
+        DevBuf sbuckets, items, part, defs;          // descriptors, sweep items, split products
+        DevBuf bbitmap, bsegcount, boffs, bkeys, blos;   // columns above 2^32: bitmaps and their keys
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        bool inflight = false;
+        std::vector<SReq*> finishing;                // their lift runs right after this step
+        uint32_t dirty_top = 1u << 30;               // device descriptors at or above: all nsplit = 0
+    } slot[2];
+    int cur = 0;
     std::vector<SBucket> sb;
     std::vector<Bucket> pdesc;                 // persistent descriptors (device copy: pbuckets)
     RowPool pool;                              // rows of the device row pool
@@ -106,6 +128,9 @@ struct wl_server {
     std::vector<SReq*> active;                 // scheduler thread only
     std::thread worker;
     bool stop = false;
+    // something may let queued requests in: a submit, a cancel, rows freed
+    // (under mu); admission is tried only then, since it drains the pipeline
+    bool admit_pending = false;
     uint64_t next_id = 1;
     wl_server_stats stats = {};    // published copy (under mu)
     wl_server_stats ws = {};       // scheduler thread's own
@@ -117,6 +142,7 @@ struct wl_server {
 };
 
 static void serve_release(wl_server* s, SReq* q) {
+    s->admit_pending = true;
     for (uint32_t bid : q->bids) {
         s->sb[bid] = SBucket();
         memset(&s->pdesc[bid], 0, sizeof(Bucket));
@@ -361,35 +387,103 @@ static void serve_admit_batch(wl_server* s, const std::vector<SReq*>& cands, std
     s->ws.ms_admit += ms;
 }
 
-// One scheduler step: every bucket with columns left advances by one chunk.
-static int serve_step_run(wl_server* s);
-static int serve_step(wl_server* s) {
-    const double t = s->now_ms();
-    const int e = serve_step_run(s);
-    s->ws.ms_wall_steps += s->now_ms() - t;
-    return e;
-}
-static int serve_step_run(wl_server* s) {
+// Requests whose every bucket is done: their lift (k_finish over the merged
+// running products) is queued behind the step, and the step's end recorded.
+static int serve_queue_finishes(wl_server* s, wl_server::Slot& sl) {
     wl_ctx* c = s->c;
+    for (SReq* q : s->active) {
+        if (q->finishing || q->cancel_seen) continue;
+        bool done = true;
+        for (uint32_t bid : q->bids) done &= s->sb[bid].done();
+        if (!done) continue;
+        launch_finish(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), nullptr, nullptr, 1,
+                      nullptr, q->r0, q->nrows, q->qcap == 0 ? 1 : 0, as<RowOut>(s->out), c->st, as<uint4>(s->acc),
+                      as<Deficit>(s->bdef), nullptr, nullptr);
+        s->ws.launches++;
+        q->finishing = true;
+        sl.finishing.push_back(q);
+    }
+    cudaEventRecord(sl.e1, c->st);
+    CK(cudaGetLastError());
+    sl.inflight = true;
+    return 0;
+}
+
+// One scheduler step, queued without waiting: every bucket with columns left
+// advances by one chunk, then the lift of the requests that are done.
+static int serve_step(wl_server* s) {
+    wl_ctx* c = s->c;
+    wl_server::Slot& sl = s->slot[s->cur];      // not in flight: the loop completes it first
     // kind 0: sparse columns of the resident table, 1: dense ones, 2: a chunk of
     // the number line above 2^32 (integers [c0, c0 + len), sieved this step)
     struct Work { uint32_t bid; uint64_t c0, len; int kind; };
     std::vector<Work> work;
-    // the step's descriptor table covers every slot (a merge over a span of
-    // rows may meet stale bucket ids of freed rows): slots without work this
-    // step have nsplit = 0
-    const uint32_t top = s->bucket_cap;
+    // The step's descriptor table covers every slot a merge may meet (a merge
+    // over a span of rows may meet stale bucket ids of freed rows): slots
+    // without work this step have nsplit = 0.  Slots are handed out lowest
+    // first, so the active ones lie below `top`; the device table is written
+    // up to max(top, what this set of buffers held before), so that no entry
+    // above `top` keeps splits of an earlier step.
+    uint32_t top = 0;
+    for (SReq* q : s->active)
+        for (uint32_t bid : q->bids) top = std::max(top, bid + 1);
+    const uint32_t upload = std::min(s->bucket_cap, std::max(top, sl.dirty_top));
     size_t nact = 0;
-    for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && !s->sb[bid].done();
-    if (!nact) return 0;
-    // an equal share of the cell budget per bucket; a dense column costs
-    // about five cells (prefix fold + windowed buckets), an integer above 2^32
-    // its share of the sieve plus a cell per prime
-    const double share = (double)s->step_cells / (double)nact;
+    for (uint32_t bid = 0; bid < top; ++bid) nact += s->sb[bid].used && !s->sb[bid].idle();
+    if (!nact) {                                 // only lifts to queue
+        cudaEventRecord(sl.e0, c->st);
+        return serve_queue_finishes(s, sl);
+    }
+    // each bucket's share of the step's cell budget.  Costs in cells: a dense
+    // column about five (prefix fold + windowed buckets), an integer above 2^32
+    // its share of the sieve plus a cell per prime.  Equal shares, or shares
+    // weighted by 1 / sqrt(the request's work left), so that small requests
+    // finish in a step or two while large ones keep a floor of a quarter of an
+    // equal share; budget a bucket cannot use goes to the others.  (Measured
+    // on the 2,000-request stream: weights 1 / sqrt(work) with a quarter floor
+    // gave the steadiest tail; 1 / work with an eighth floor, or either with a
+    // half floor, and equal shares gave longer ones.)
+    auto work_left = [](const SBucket& b) {
+        double r = 0;
+        if (b.pos < b.ncols) {
+            const uint64_t dl = b.pos < b.cdense ? b.cdense - b.pos : 0;
+            const uint64_t sl = b.ncols - std::max(b.pos, b.cdense);
+            r += (double)b.nrows * (5.0 * (double)dl + (double)sl);
+        }
+        if (b.bpos < b.bend)
+            r += (double)(b.bend - b.bpos) * (BIG_SIEVE_CELLS + (double)b.nrows / std::log((double)b.bpos));
+        return r;
+    };
+    const double budget = (double)s->step_cells;
+    std::vector<double> wgt(top, 0.0), left(top, 0.0), share_of(top, 0.0);
+    double wsum = 0;
+    for (SReq* q : s->active) {
+        double R = 0;
+        for (uint32_t bid : q->bids) {
+            if (bid >= top || !s->sb[bid].used || s->sb[bid].idle()) continue;
+            left[bid] = work_left(s->sb[bid]);
+            R += left[bid];
+        }
+        for (uint32_t bid : q->bids) {
+            if (bid >= top || left[bid] <= 0) continue;
+            wgt[bid] = s->shares == WL_SHARES_EQUAL ? 1.0 : 1.0 / std::sqrt(std::max(R, 1.0));
+            wsum += wgt[bid];
+        }
+    }
+    double spare = 0, wrest = 0;
+    for (uint32_t bid = 0; bid < top; ++bid) {
+        if (wgt[bid] <= 0) continue;
+        share_of[bid] = std::max(budget * wgt[bid] / wsum, budget / (4.0 * (double)nact));
+        if (left[bid] < share_of[bid]) { spare += share_of[bid] - left[bid]; share_of[bid] = left[bid]; }
+        else wrest += wgt[bid];
+    }
+    for (uint32_t bid = 0; bid < top; ++bid)
+        if (wgt[bid] > 0 && left[bid] > share_of[bid] && wrest > 0) share_of[bid] += spare * wgt[bid] / wrest;
     double W = 0;
     for (uint32_t bid = 0; bid < top; ++bid) {
         SBucket& b = s->sb[bid];
-        if (!b.used || b.done()) continue;
+        if (!b.used || b.idle()) continue;
+        const double share = std::max(share_of[bid], 1.0);
         Work w;
         w.bid = bid;
         double per, cost;
@@ -422,7 +516,7 @@ static int serve_step_run(wl_server* s) {
         work.push_back(w);
     }
     const double target_threads = (double)c->sms * 2048.0 * 4.0;
-    std::vector<Bucket> sbk(top);
+    std::vector<Bucket> sbk(upload);
     memset(sbk.data(), 0, sbk.size() * sizeof(Bucket));
     struct Grp { int L, rpt, kind; std::vector<SweepItem> items; };
     std::vector<Grp> groups;
@@ -435,7 +529,7 @@ static int serve_step_run(wl_server* s) {
         Bucket& x = sbk[w.bid];
         x = s->pdesc[w.bid];
         int rpt = 1;
-        uint32_t tps = 256;
+        uint32_t min_tps = 1;
         uint64_t S;
         if (w.kind == 2) {
             // the chunk's bitmap region: its words from bwords on
@@ -451,7 +545,6 @@ static int serve_step_run(wl_server* s) {
             boffs_need = std::max(boffs_need, ncta * std::max<uint32_t>(b.nroot, 1));
             bseg_need = std::max(bseg_need, nseg);
             if (b.nrows >= 512) rpt = 2;
-            if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
             // splits by the sweep's cells per row: the chunk's primes, about len / ln(c0)
             S = (uint64_t)std::ceil((double)rpt * ((double)w.len / std::log((double)w.c0)) * target_threads / W);
             S = std::max<uint64_t>(1, std::min<uint64_t>(S, std::max<uint64_t>(1, nw / 256)));
@@ -462,10 +555,11 @@ static int serve_step_run(wl_server* s) {
             x.cbase = (uint32_t)w.c0;
             x.ncols = (uint32_t)w.len;
             if (dense) {
-                dense_shape(b.nrows, &rpt, &tps);
+                uint32_t dtps;
+                dense_shape(b.nrows, &rpt, &dtps);
+                min_tps = 8;
             } else {
                 rpt = sparse_rpt_for(c->tune.sparse_rpt[b.L - 2], b.nrows);
-                if (b.nrows < 256) { tps = 1; while (tps < b.nrows) tps <<= 1; }
             }
             const double per = (double)b.nrows * (dense ? 5.0 : 1.0);
             S = (uint64_t)std::ceil((double)rpt * per / (double)b.nrows * (double)w.len * target_threads / W);
@@ -482,41 +576,41 @@ static int serve_step_run(wl_server* s) {
         part_total += S * b.nrows;
         def_total += (uint32_t)S;
         bucket_splits[w.bid] = (uint32_t)S;
-        Grp* g = nullptr;
-        for (auto& gg : groups)
-            if (gg.L == (int)b.L && gg.rpt == rpt && gg.kind == w.kind) g = &gg;
-        if (!g) {
-            groups.push_back({ (int)b.L, rpt, w.kind, {} });
-            g = &groups.back();
-        }
-        if (tps == 256) {
-            const uint32_t tile = 256 * rpt;
-            for (uint32_t r = 0; r < b.nrows; r += tile)
-                for (uint32_t s2 = 0; s2 < S; ++s2) g->items.push_back({ w.bid, r, s2, 256u });
-        } else {
-            const uint32_t per_cta = 256 / tps;
-            for (uint32_t s2 = 0; s2 < S; s2 += per_cta) g->items.push_back({ w.bid, 0, s2, tps });
+        std::vector<RowTile> tiles;
+        row_tiles(b.nrows, rpt, min_tps, tiles, w.kind == 1);
+        for (const RowTile& t : tiles) {
+            Grp* g = nullptr;
+            for (auto& gg : groups)
+                if (gg.L == (int)b.L && gg.rpt == t.rpt && gg.kind == w.kind) g = &gg;
+            if (!g) {
+                groups.push_back({ (int)b.L, t.rpt, w.kind, {} });
+                g = &groups.back();
+            }
+            tile_items(t, 0, (uint32_t)S, [&](uint32_t r0, uint32_t s2, uint32_t tp) {
+                g->items.push_back({ w.bid, r0, s2, tp });
+            });
         }
     }
     std::vector<SweepItem> all;
     for (auto& g : groups) all.insert(all.end(), g.items.begin(), g.items.end());
-    RC(ensure(s->sbuckets, sbk.size() * sizeof(Bucket)));
-    RC(ensure(c->items, all.size() * sizeof(SweepItem) + 16));
-    RC(ensure(c->part, part_total * 16 + 16));
-    RC(ensure(c->defs, (size_t)def_total * sizeof(Deficit) + 16));
+    RC(ensure(sl.sbuckets, (size_t)s->bucket_cap * sizeof(Bucket)));
+    RC(ensure(sl.items, all.size() * sizeof(SweepItem) + 16));
+    RC(ensure(sl.part, part_total * 16 + 16));
+    RC(ensure(sl.defs, (size_t)def_total * sizeof(Deficit) + 16));
     if (bwords) {
-        RC(ensure(s->bbitmap, bwords * 4));
-        RC(ensure(s->bsegcount, bseg_need * 4 + 16));
-        RC(ensure(s->boffs, boffs_need * 4 + 16));
-        RC(ensure(s->bkeys, (size_t)top * 8));
-        RC(ensure(s->blos, (size_t)top * 8));
+        RC(ensure(sl.bbitmap, bwords * 4));
+        RC(ensure(sl.bsegcount, bseg_need * 4 + 16));
+        RC(ensure(sl.boffs, boffs_need * 4 + 16));
+        RC(ensure(sl.bkeys, (size_t)s->bucket_cap * 8));
+        RC(ensure(sl.blos, (size_t)s->bucket_cap * 8));
     }
-    cudaEventRecord(s->e0, c->st);
-    CK(cudaMemcpyAsync(s->sbuckets.p, sbk.data(), sbk.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->items.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, c->st));
+    cudaEventRecord(sl.e0, c->st);
+    CK(cudaMemcpyAsync(sl.sbuckets.p, sbk.data(), sbk.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
+    sl.dirty_top = top;
+    CK(cudaMemcpyAsync(sl.items.p, all.data(), all.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, c->st));
     if (bwords) {
-        CK(cudaMemcpyAsync(s->bkeys.p, bkeys.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(s->blos.p, blos.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(sl.bkeys.p, bkeys.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(sl.blos.p, blos.data(), (size_t)top * 8, cudaMemcpyHostToDevice, c->st));
         // sieve every chunk above 2^32 into its bitmap region (the sieving
         // primes 67 .. sqrt(key) come from the resident column table; one
         // launch after another on the stream, so they share the offsets)
@@ -525,27 +619,27 @@ static int serve_step_run(wl_server* s) {
             const SBucket& b = s->sb[w.bid];
             const uint32_t nseg = (uint32_t)(w.len / BIG_SPAN);
             launch_sieve_big(w.c0, std::min(w.c0 + w.len, b.bend), nseg, 8, as<uint32_t>(c->cols) + 18, b.nroot,
-                             as<uint32_t>(s->boffs), as<uint32_t>(s->bbitmap) + sbk[w.bid].cbase,
-                             as<uint32_t>(s->bsegcount), c->st);
+                             as<uint32_t>(sl.boffs), as<uint32_t>(sl.bbitmap) + sbk[w.bid].cbase,
+                             as<uint32_t>(sl.bsegcount), c->st);
             s->ws.launches++;
         }
     }
     size_t ioff = 0;
     for (auto& g : groups) {
         if (g.kind == 2)
-            launch_sweep_bits(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
-                              as<SweepItem>(c->items) + ioff, as<RowMod>(s->mods), as<uint32_t>(s->bbitmap), 0,
-                              as<uint64_t>(s->bkeys), as<uint4>(c->part), as<Deficit>(c->defs), c->st,
-                              as<uint64_t>(s->blos));
+            launch_sweep_bits(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(sl.sbuckets),
+                              as<SweepItem>(sl.items) + ioff, as<RowMod>(s->mods), as<uint32_t>(sl.bbitmap), 0,
+                              as<uint64_t>(sl.bkeys), as<uint4>(sl.part), as<Deficit>(sl.defs), c->st,
+                              as<uint64_t>(sl.blos));
         else if (g.kind == 1)
-            launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets), as<SweepItem>(c->items) + ioff,
-                               as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(c->part),
-                               as<Deficit>(c->defs), c->st,
+            launch_sweep_dense(g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(sl.sbuckets), as<SweepItem>(sl.items) + ioff,
+                               as<RowMod>(s->mods), as<uint32_t>(c->cols), nullptr, as<uint4>(sl.part),
+                               as<Deficit>(sl.defs), c->st,
                                c->tune.dense_kernel[g.L - 2], (uint32_t)c->tune.dense_hstep[g.L - 2]);
         else
-            launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(s->sbuckets),
-                         as<SweepItem>(c->items) + ioff, as<RowMod>(s->mods), as<uint32_t>(c->cols),
-                         as<uint4>(c->part), as<Deficit>(c->defs), c->st);
+            launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(sl.sbuckets),
+                         as<SweepItem>(sl.items) + ioff, as<RowMod>(s->mods), as<uint32_t>(c->cols),
+                         as<uint4>(sl.part), as<Deficit>(sl.defs), c->st);
         s->ws.launches++;
         ioff += g.items.size();
     }
@@ -565,49 +659,34 @@ static int serve_step_run(wl_server* s) {
         }
         if (!maxs) continue;
         if (maxs >= (uint32_t)c->tune.merge_cta_min)
-            launch_merge_cta(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
-                             as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
+            launch_merge_cta(L, as<Bucket>(sl.sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                             as<uint4>(sl.part), as<Deficit>(sl.defs), lo, hi - lo, as<uint4>(s->acc),
                              as<Deficit>(s->bdef), c->st);
         else
-            launch_merge(L, as<Bucket>(s->sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
-                         as<uint4>(c->part), as<Deficit>(c->defs), lo, hi - lo, as<uint4>(s->acc),
+            launch_merge(L, as<Bucket>(sl.sbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods),
+                         as<uint4>(sl.part), as<Deficit>(sl.defs), lo, hi - lo, as<uint4>(s->acc),
                          as<Deficit>(s->bdef), c->st);
         s->ws.launches++;
     }
-    cudaEventRecord(s->e1, c->st);
-    CK(cudaStreamSynchronize(c->st));
-    CK(cudaGetLastError());
-    float ms = 0;
-    cudaEventElapsedTime(&ms, s->e0, s->e1);
-    s->ws.ms_steps += ms;
-    s->ws.steps++;
+    // positions advance now, so the next step is planned while this one runs
     for (const Work& w : work) {
         SBucket& b = s->sb[w.bid];
         if (w.kind == 2) b.bpos = std::min(w.c0 + w.len, b.bend);
         else b.pos += w.len;
     }
-    return 0;
+    return serve_queue_finishes(s, sl);
 }
 
-static int serve_finish_run(wl_server* s, SReq* q);
-static int serve_finish(wl_server* s, SReq* q) {
-    const double t = s->now_ms();
-    const int e = serve_finish_run(s, q);
-    s->ws.ms_wall_finish += s->now_ms() - t;
-    return e;
-}
-static int serve_finish_run(wl_server* s, SReq* q) {
+// The rows of a request whose lift has run (the step it followed is
+// complete): read them back, in ascending p, with the checksum and the
+// result lines (cl_wilson.cpp:872-900).
+static int serve_read_rows(wl_server* s, SReq* q) {
     wl_ctx* c = s->c;
     const bool full = q->qcap == 0;
-    launch_finish(q->L, as<Bucket>(s->pbuckets), as<RowInfo>(s->info), as<RowMod>(s->mods), nullptr, nullptr, 1,
-                  nullptr, q->r0, q->nrows, full ? 1 : 0, as<RowOut>(s->out), c->st, as<uint4>(s->acc),
-                  as<Deficit>(s->bdef), nullptr, nullptr);
-    s->ws.launches++;
     std::vector<RowOut> ro(q->nrows);
     CK(cudaMemcpyAsync(ro.data(), as<RowOut>(s->out) + q->r0, (size_t)q->nrows * sizeof(RowOut),
-                       cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    CK(cudaGetLastError());
+                       cudaMemcpyDeviceToHost, c->st3));
+    CK(cudaStreamSynchronize(c->st3));
     std::vector<uint32_t> ord(q->nrows);
     for (uint32_t k = 0; k < q->nrows; ++k) ord[k] = k;
     std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return q->primes[a] < q->primes[b]; });
@@ -654,16 +733,54 @@ static void serve_end(wl_server* s, SReq* q, int state, int rc) {
     s->cv_done.notify_all();
 }
 
+// Ends a request that is in s->active: frees its rows and slots and removes it.
+static void serve_retire(wl_server* s, SReq* q, int state, int rc) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    serve_release(s, q);
+    serve_end(s, q, state, rc);
+    s->active.erase(std::find(s->active.begin(), s->active.end(), q));
+}
+
+// Waits for the step in `sl`, takes its device time, and completes the
+// requests whose lift followed it.  err != 0 (a failed step) fails them.
+static void serve_complete(wl_server* s, wl_server::Slot& sl, int err = 0) {
+    if (!sl.inflight) return;
+    const double t = s->now_ms();
+    if (!err && cudaEventSynchronize(sl.e1) != cudaSuccess) err = WL_ERR_CUDA;
+    if (!err) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, sl.e0, sl.e1);
+        s->ws.ms_steps += ms;
+        s->ws.steps++;
+    }
+    for (SReq* q : sl.finishing) {
+        const int rc = err ? err : serve_read_rows(s, q);
+        serve_retire(s, q, rc ? WL_REQ_FAILED : WL_REQ_DONE, rc);
+    }
+    sl.finishing.clear();
+    sl.inflight = false;
+    s->ws.ms_wall_finish += s->now_ms() - t;
+}
+
+// Completes every step in flight, the older first: the stream is then idle.
+static void serve_drain(wl_server* s, int err = 0) {
+    serve_complete(s, s->slot[s->cur], err);       // the older of the two, if both are in flight
+    serve_complete(s, s->slot[s->cur ^ 1], err);
+    if (err) cudaGetLastError();
+}
+
 static void serve_loop(wl_server* s) {
     cudaSetDevice(s->c->device);
     while (true) {
-        // admit queued requests in FIFO order while they fit, all at once
-        std::vector<SReq*> cands;
+        // queued requests to admit (cancelled ones end here), and cancelled active ones
+        std::vector<SReq*> cands, cancelled;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            while (!s->stop && s->queue.empty() && s->active.empty()) s->cv_work.wait(lk);
-            if (s->stop) return;
-            for (auto it = s->queue.begin(); it != s->queue.end();) {
+            while (!s->stop && s->active.empty() && !(s->admit_pending && !s->queue.empty())) s->cv_work.wait(lk);
+            if (s->stop) break;
+            const bool try_admit = s->admit_pending;
+            s->admit_pending = false;
+            for (auto it = s->queue.begin(); it != s->queue.end() && try_admit;) {
                 if ((*it)->cancel) {
                     serve_end(s, *it, WL_REQ_CANCELLED, 0);
                     it = s->queue.erase(it);
@@ -672,8 +789,21 @@ static void serve_loop(wl_server* s) {
                     ++it;
                 }
             }
+            for (SReq* q : s->active)
+                if (q->cancel && !q->finishing && !q->cancel_seen) cancelled.push_back(q);
+        }
+        if (!cancelled.empty()) {
+            // no step may still use their rows: drain, then free them
+            serve_drain(s);
+            for (SReq* q : cancelled) {
+                q->cancel_seen = true;
+                for (uint32_t bid : q->bids) s->sb[bid].stop = true;
+                serve_retire(s, q, WL_REQ_CANCELLED, 0);
+            }
         }
         if (!cands.empty()) {
+            // admission synchronises the stream and may grow the column table
+            serve_drain(s);
             std::vector<int> res;
             const double t = s->now_ms();
             serve_admit_batch(s, cands, res);
@@ -698,28 +828,30 @@ static void serve_loop(wl_server* s) {
             s->ws.peak_active = std::max<uint32_t>(s->ws.peak_active, (uint32_t)s->active.size());
             s->stats = s->ws;
         }
-        if (s->active.empty()) continue;
-        const int e = serve_step(s);
-        std::vector<SReq*> keep;
-        for (SReq* q : s->active) {
-            bool done = true;
-            for (uint32_t bid : q->bids) done &= s->sb[bid].done();
-            bool cancel;
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                cancel = q->cancel;
+        // queue the next step into the free set of buffers, then complete the
+        // previous step while this one runs
+        bool work = false;                           // chunks to sweep or lifts to queue
+        for (SReq* q : s->active) work |= !q->finishing && !q->cancel_seen;
+        if (work) {
+            serve_complete(s, s->slot[s->cur]);
+            const double t = s->now_ms();
+            const int e = serve_step(s);
+            s->ws.ms_wall_steps += s->now_ms() - t;
+            if (e) {
+                // a failed step: every request still running fails with its code
+                serve_drain(s, e);
+                std::vector<SReq*> all(s->active);
+                for (SReq* q : all) serve_retire(s, q, WL_REQ_FAILED, e);
+                continue;
             }
-            if (!e && !cancel && !done) { keep.push_back(q); continue; }
-            int rc = e;
-            if (!e && !cancel) rc = serve_finish(s, q);
-            std::lock_guard<std::mutex> lk(s->mu);
-            serve_release(s, q);
-            serve_end(s, q, cancel ? WL_REQ_CANCELLED : (rc ? WL_REQ_FAILED : WL_REQ_DONE), cancel ? 0 : rc);
         }
+        serve_complete(s, s->slot[s->cur ^ 1]);
+        if (work) s->cur ^= 1;
+        else serve_complete(s, s->slot[s->cur]);
         std::lock_guard<std::mutex> lk(s->mu);
-        s->active.swap(keep);
         s->stats = s->ws;
     }
+    serve_drain(s);
 }
 
 extern "C" {
@@ -742,6 +874,12 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
     }
     s->pool_cap = (uint32_t)std::min<uint64_t>(bytes / WL_SERVER_ROW_BYTES, 1u << 30);
     s->step_cells = o.step_cells ? o.step_cells : (1ull << 32);
+    if (o.shares > WL_SHARES_EQUAL) {
+        wl_close(s->c);
+        delete s;
+        return WL_ERR_ARG;
+    }
+    s->shares = o.shares;
     s->bucket_cap = 3 * 1024;
     s->sb.assign(s->bucket_cap, SBucket());
     s->pdesc.resize(s->bucket_cap);
@@ -751,7 +889,9 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
     if (ensure(s->info, (size_t)s->pool_cap * sizeof(RowInfo)) || ensure(s->mods, (size_t)s->pool_cap * sizeof(RowMod)) ||
         ensure(s->acc, (size_t)s->pool_cap * 16) || ensure(s->out, (size_t)s->pool_cap * sizeof(RowOut)) ||
         ensure(s->pbuckets, s->bucket_cap * sizeof(Bucket)) || ensure(s->bdef, s->bucket_cap * sizeof(Deficit)) ||
-        cudaEventCreate(&s->e0) != cudaSuccess || cudaEventCreate(&s->e1) != cudaSuccess) {
+        cudaEventCreate(&s->e0) != cudaSuccess || cudaEventCreate(&s->e1) != cudaSuccess ||
+        cudaEventCreate(&s->slot[0].e0) != cudaSuccess || cudaEventCreate(&s->slot[0].e1) != cudaSuccess ||
+        cudaEventCreate(&s->slot[1].e0) != cudaSuccess || cudaEventCreate(&s->slot[1].e1) != cudaSuccess) {
         cudaGetLastError();
         DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->bdef };
         for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
@@ -778,6 +918,7 @@ int wl_server_submit(wl_server* s, uint64_t pmin, uint64_t pmax, uint64_t q_cap,
     q->t_submit = s->now_ms();
     s->reqs[q->id] = q;
     s->queue.push_back(q);
+    s->admit_pending = true;
     if (id) *id = q->id;
     s->cv_work.notify_all();
     return 0;
@@ -855,6 +996,7 @@ int wl_server_cancel(wl_server* s, uint64_t id) {
     SReq* q = find_req(s, id);
     if (!q) return WL_ERR_ARG;
     q->cancel = true;
+    s->admit_pending = true;
     s->cv_work.notify_all();
     return 0;
 }
@@ -886,9 +1028,15 @@ void wl_server_close(wl_server* s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->c->device);
     cudaStreamSynchronize(s->c->st);
-    DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->sbuckets, &s->bdef, &s->ipart,
-                       &s->bbitmap, &s->bsegcount, &s->boffs, &s->bkeys, &s->blos };
+    DevBuf* bufs[] = { &s->info, &s->mods, &s->acc, &s->out, &s->pbuckets, &s->bdef, &s->ipart };
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    for (auto& sl : s->slot) {
+        DevBuf* sb[] = { &sl.sbuckets, &sl.items, &sl.part, &sl.defs, &sl.bbitmap, &sl.bsegcount, &sl.boffs,
+                         &sl.bkeys, &sl.blos };
+        for (DevBuf* b : sb) if (b->p) cudaFree(b->p);
+        if (sl.e0) cudaEventDestroy(sl.e0);
+        if (sl.e1) cudaEventDestroy(sl.e1);
+    }
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);
     for (auto& kv : s->reqs) delete kv.second;

@@ -233,6 +233,7 @@ int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p
 #define WL_DENSE_SWITCH_W4 3   /* per-column bucket switch, 4-bit, 2 CTAs/SM */
 #define WL_DENSE_SMEM_W3   4   /* digit-sorted, buckets in shared memory, 3-bit, 4 CTAs/SM */
 #define WL_DENSE_SMEM_W4   5   /* digit-sorted, buckets in shared memory, 4-bit, 2 CTAs/SM */
+#define WL_DENSE_SORTED_W3_2CTA 6   /* digit-sorted windows, 3-bit, 2 CTAs/SM (no register spills) */
 typedef struct {
     int32_t sparse_variant[3];   /* cell formulation of the prefix-fold sweep: 0 carry chain, 1 wide products,
                                     2 high half first, 3 wide products with each thread's last row on the carry chain */
@@ -277,9 +278,11 @@ int wl_autotune(wl_ctx *ctx, const wl_range *ranges, size_t n, uint64_t q_cap, u
  * whole pool fails with WL_ERR_NOMEM.  All functions are thread-safe. */
 typedef struct wl_server wl_server;
 
+#define WL_SHARES_LEAST_WORK 0   /* shares weighted by 1/sqrt(work left): small requests first, large ones keep moving */
+#define WL_SHARES_EQUAL      1   /* every active (request, class) bucket gets an equal share */
 typedef struct {
     int device;
-    uint32_t pad;
+    uint32_t shares;       /* WL_SHARES_*: how a step's cell budget is split between requests */
     uint64_t pool_bytes;   /* device memory for resident rows (0: 1 GiB); WL_SERVER_ROW_BYTES each */
     uint64_t step_cells;   /* column-cell budget of one scheduler step (0: 2^32) */
     const wl_tuning *tuning;   /* kernel choices (NULL: the defaults) */
@@ -317,9 +320,9 @@ typedef struct {
     double ms_admit;       /* device time of admissions */
     uint32_t peak_rows;    /* largest number of resident rows */
     uint32_t peak_active;  /* largest number of admitted requests at once */
-    double ms_wall_steps;  /* scheduler wall time in steps: planning, uploads, launches, waiting */
-    double ms_wall_admit;  /* scheduler wall time in admissions */
-    double ms_wall_finish; /* scheduler wall time finishing requests (lift, read-back, result lines) */
+    double ms_wall_steps;  /* scheduler wall time planning and queueing steps (overlaps the previous step) */
+    double ms_wall_admit;  /* scheduler wall time in admissions (the pipeline drained first) */
+    double ms_wall_finish; /* scheduler wall time waiting for steps to end and completing requests */
 } wl_server_stats;
 
 int wl_server_open(const wl_server_opts *opts, wl_server **out);

@@ -57,10 +57,10 @@ def test_alone(expected):
             srv.release(rid)
 
 
-@pytest.mark.parametrize("step_cells", [0, 1 << 24])
-def test_mixed(expected, step_cells):
+@pytest.mark.parametrize("step_cells,shares", [(0, "least-work"), (1 << 24, "least-work"), (1 << 24, "equal")])
+def test_mixed(expected, step_cells, shares):
     # everything at once, and a second wave submitted while the first runs
-    with wl.Server(0, step_cells=step_cells) as srv:
+    with wl.Server(0, step_cells=step_cells, shares=shares) as srv:
         keys = _all_keys()
         ids = [srv.submit(*k) for k in keys]
         ids2 = [srv.submit(*k) for k in reversed(keys)]

@@ -779,6 +779,8 @@ def main():
         "mulmods_per_s": cells_all / tot_dev,
         "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_mad / 1e12, "unit": "TOP/s",
                      "frac": achieved * 1e12 / peak_mad, "traffic": traffic,
+                     "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of the step's sweep launches of "
+                                        "this workload, one ncu capture (profiles/traffic.json)") if traffic else None,
                      "kernel": f"k_sweep<{L},*>" if dense_cells < 0.5 * exec_cells else f"k_sweep_dense<{L},*>",
                      "ops_per_cell": OPS_PER_CELL[L],
                      "cells_executed_per_step": exec_cells / args.steps,

@@ -529,12 +529,21 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     uint64_t part_total = 0;
     uint32_t def_total = 0;
     out.cells = 0;
-    struct ItemGroup { int L, rpt; bool dense; std::vector<SweepItem> items; };
+    // sweep items per launch, with each item's modelled cost (rows x cells per
+    // row of its splits): a launch runs its items longest first, so that the
+    // last CTAs to start are short ones
+    struct ItemGroup { int L, rpt; bool dense; std::vector<SweepItem> items; std::vector<double> cost; };
     std::vector<ItemGroup> groups;
-    auto group_for = [&](int L, int rpt, bool dense) -> std::vector<SweepItem>& {
-        for (auto& g : groups) if (g.L == L && g.rpt == rpt && g.dense == dense) return g.items;
-        groups.push_back({ L, rpt, dense, {} });
-        return groups.back().items;
+    auto group_for = [&](int L, int rpt, bool dense) -> ItemGroup& {
+        for (auto& g : groups) if (g.L == L && g.rpt == rpt && g.dense == dense) return g;
+        groups.push_back({ L, rpt, dense, {}, {} });
+        return groups.back();
+    };
+    // rows one item of a tile covers, times the splits it holds
+    auto item_rows = [](const RowTile& t, uint32_t nrows) -> double {
+        const uint32_t left = nrows - t.row0;
+        const uint32_t span = t.tps * (uint32_t)t.rpt;
+        return (double)(left < span ? left : span) * (t.tps == 256 ? 1.0 : (double)(256 / t.tps));
     };
     // splits per bucket (wl_plan.h), lengthened when the split partials would
     // not fit a third of the free device memory (24 GiB at most)
@@ -593,22 +602,30 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         out.cells += (uint64_t)b.nrows * b.ncols;
         std::vector<RowTile> tiles;
         if (Ss) {
+            const double per_split = (double)(b.ncols - b.cdense) / (double)Ss;   // sparse: equal splits
             row_tiles(b.nrows, rpt, 1, tiles);
             for (const RowTile& t : tiles) {
-                auto& items = group_for((int)b.L, t.rpt, false);
-                tile_items(t, (uint32_t)Sd, (uint32_t)S,
-                           [&](uint32_t r0, uint32_t s2, uint32_t tp) { items.push_back({ oi, r0, s2, tp }); });
+                ItemGroup& g = group_for((int)b.L, t.rpt, false);
+                const double c = per_split * item_rows(t, b.nrows);
+                tile_items(t, (uint32_t)Sd, (uint32_t)S, [&](uint32_t r0, uint32_t s2, uint32_t tp) {
+                    g.items.push_back({ oi, r0, s2, tp });
+                    g.cost.push_back(c);
+                });
             }
         }
         if (Sd) {
             int drpt;
             uint32_t dtps;
             dense_shape(b.nrows, &drpt, &dtps);
+            const double per_split = dcost[i] / (double)Sd;   // dense: splits of equal modelled cost
             row_tiles(b.nrows, drpt, 8, tiles, true);
             for (const RowTile& t : tiles) {
-                auto& items = group_for((int)b.L, t.rpt, true);
-                tile_items(t, 0, (uint32_t)Sd,
-                           [&](uint32_t r0, uint32_t s2, uint32_t tp) { items.push_back({ oi, r0, s2, tp }); });
+                ItemGroup& g = group_for((int)b.L, t.rpt, true);
+                const double c = per_split * item_rows(t, b.nrows);
+                tile_items(t, 0, (uint32_t)Sd, [&](uint32_t r0, uint32_t s2, uint32_t tp) {
+                    g.items.push_back({ oi, r0, s2, tp });
+                    g.cost.push_back(c);
+                });
             }
         }
         for (uint32_t k = 0; k < b.nrows; ++k) {
@@ -703,7 +720,12 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     CK(cudaMemcpyAsync(c->rowinfo.p, ri.data(), (size_t)nrows * sizeof(RowInfo), cudaMemcpyHostToDevice, c->st));
     std::vector<SweepItem> all_items;
     all_items.reserve(nitems_total);
-    for (auto& g : groups) all_items.insert(all_items.end(), g.items.begin(), g.items.end());
+    for (auto& g : groups) {
+        std::vector<uint32_t> ord(g.items.size());
+        for (uint32_t k = 0; k < ord.size(); ++k) ord[k] = k;
+        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b2) { return g.cost[a] > g.cost[b2]; });
+        for (uint32_t k : ord) all_items.push_back(g.items[k]);
+    }
     if (!all_items.empty())
         CK(cudaMemcpyAsync(c->items.p, all_items.data(), all_items.size() * sizeof(SweepItem),
                            cudaMemcpyHostToDevice, c->st));

@@ -135,11 +135,42 @@ struct wl_server {
     wl_server_stats stats = {};    // published copy (under mu)
     wl_server_stats ws = {};       // scheduler thread's own
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaMemPool_t mpool = nullptr;   // the step buffers' stream-ordered pool
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
 };
+
+// A step buffer of at least `bytes`.  Step buffers come from the session's own
+// stream-ordered pool: one that must grow is freed and reallocated in the
+// order of the main stream, behind the step in flight, so the host does not
+// wait for that step (cudaFree would wait for the whole device: tens of
+// milliseconds, at times more, with the GPU idle until the next step is
+// queued), and the pool keeps freed memory for the next growth instead of
+// handing it back to the driver.  A buffer grows to half as much again as its
+// old size, or to `bytes` if more.
+static int ensure_step(wl_server* s, DevBuf& b, size_t bytes) {
+    if (bytes <= b.cap && b.p) return 0;
+    cudaStream_t st = s->c->st;
+    const size_t want = std::max<size_t>(bytes, 256);
+    const size_t grown = std::max(want, b.cap + b.cap / 2);
+    if (b.p) cudaFreeAsync(b.p, st);
+    b.p = nullptr;
+    b.cap = 0;
+    if (cudaMallocFromPoolAsync(&b.p, grown, s->mpool, st) == cudaSuccess) {
+        b.cap = grown;
+        return 0;
+    }
+    cudaGetLastError();
+    if (grown != want && cudaMallocFromPoolAsync(&b.p, want, s->mpool, st) == cudaSuccess) {
+        b.cap = want;
+        return 0;
+    }
+    cudaGetLastError();
+    b.p = nullptr;
+    return WL_ERR_NOMEM;
+}
 
 static void serve_release(wl_server* s, SReq* q) {
     s->admit_pending = true;
@@ -593,16 +624,16 @@ static int serve_step(wl_server* s) {
     }
     std::vector<SweepItem> all;
     for (auto& g : groups) all.insert(all.end(), g.items.begin(), g.items.end());
-    RC(ensure(sl.sbuckets, (size_t)s->bucket_cap * sizeof(Bucket)));
-    RC(ensure(sl.items, all.size() * sizeof(SweepItem) + 16));
-    RC(ensure(sl.part, part_total * 16 + 16));
-    RC(ensure(sl.defs, (size_t)def_total * sizeof(Deficit) + 16));
+    RC(ensure_step(s, sl.sbuckets, (size_t)s->bucket_cap * sizeof(Bucket)));
+    RC(ensure_step(s, sl.items, all.size() * sizeof(SweepItem) + 16));
+    RC(ensure_step(s, sl.part, part_total * 16 + 16));
+    RC(ensure_step(s, sl.defs, (size_t)def_total * sizeof(Deficit) + 16));
     if (bwords) {
-        RC(ensure(sl.bbitmap, bwords * 4));
-        RC(ensure(sl.bsegcount, bseg_need * 4 + 16));
-        RC(ensure(sl.boffs, boffs_need * 4 + 16));
-        RC(ensure(sl.bkeys, (size_t)s->bucket_cap * 8));
-        RC(ensure(sl.blos, (size_t)s->bucket_cap * 8));
+        RC(ensure_step(s, sl.bbitmap, bwords * 4));
+        RC(ensure_step(s, sl.bsegcount, bseg_need * 4 + 16));
+        RC(ensure_step(s, sl.boffs, boffs_need * 4 + 16));
+        RC(ensure_step(s, sl.bkeys, (size_t)s->bucket_cap * 8));
+        RC(ensure_step(s, sl.blos, (size_t)s->bucket_cap * 8));
     }
     cudaEventRecord(sl.e0, c->st);
     CK(cudaMemcpyAsync(sl.sbuckets.p, sbk.data(), sbk.size() * sizeof(Bucket), cudaMemcpyHostToDevice, c->st));
@@ -899,6 +930,29 @@ int wl_server_open(const wl_server_opts* opts, wl_server** out) {
         delete s;
         return WL_ERR_NOMEM;
     }
+    // the step buffers' pool, which keeps what is freed into it; each set of
+    // step buffers starts at the size a step of the default budget takes
+    // (about two rows of split products per thread of the sweep, a split
+    // deficit per thread, a few thousand items)
+    cudaMemPoolProps pp;
+    memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = s->c->device;
+    const uint64_t keep_all = ~0ull;
+    bool ok = cudaMemPoolCreate(&s->mpool, &pp) == cudaSuccess &&
+              cudaMemPoolSetAttribute(s->mpool, cudaMemPoolAttrReleaseThreshold, (void*)&keep_all) == cudaSuccess;
+    const size_t threads = (size_t)s->c->sms * 2048 * 4;
+    for (auto& sl : s->slot)
+        ok = ok && !ensure_step(s, sl.sbuckets, (size_t)s->bucket_cap * sizeof(Bucket)) &&
+             !ensure_step(s, sl.part, threads * 2 * 16) && !ensure_step(s, sl.items, 16384 * sizeof(SweepItem)) &&
+             !ensure_step(s, sl.defs, threads * sizeof(Deficit));
+    if (!ok) {
+        cudaGetLastError();
+        wl_server_close(s);                              // no worker yet: frees what there is
+        return WL_ERR_NOMEM;
+    }
     cudaMemset(s->pbuckets.p, 0, s->bucket_cap * sizeof(Bucket));
     cudaMemset(s->info.p, 0, (size_t)s->pool_cap * sizeof(RowInfo));   // bucket 0 for rows never admitted
     s->worker = std::thread(serve_loop, s);
@@ -1033,10 +1087,12 @@ void wl_server_close(wl_server* s) {
     for (auto& sl : s->slot) {
         DevBuf* sb[] = { &sl.sbuckets, &sl.items, &sl.part, &sl.defs, &sl.bbitmap, &sl.bsegcount, &sl.boffs,
                          &sl.bkeys, &sl.blos };
-        for (DevBuf* b : sb) if (b->p) cudaFree(b->p);
+        for (DevBuf* b : sb) if (b->p) cudaFreeAsync(b->p, s->c->st);
         if (sl.e0) cudaEventDestroy(sl.e0);
         if (sl.e1) cudaEventDestroy(sl.e1);
     }
+    cudaStreamSynchronize(s->c->st);
+    if (s->mpool) cudaMemPoolDestroy(s->mpool);
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);
     for (auto& kv : s->reqs) delete kv.second;

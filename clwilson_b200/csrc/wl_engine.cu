@@ -543,7 +543,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     auto item_rows = [](const RowTile& t, uint32_t nrows) -> double {
         const uint32_t left = nrows - t.row0;
         const uint32_t span = t.tps * (uint32_t)t.rpt;
-        return (double)(left < span ? left : span) * (t.tps == 256 ? 1.0 : (double)(256 / t.tps));
+        return (double)(left < span ? left : span) * (double)tile_groups(t);
     };
     // splits per bucket (wl_plan.h), lengthened when the split partials would
     // not fit a third of the free device memory (24 GiB at most)

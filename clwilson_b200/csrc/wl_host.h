@@ -47,43 +47,49 @@ inline int sparse_rpt_for(int tuned, uint32_t nrows) {
 // above: several splits share a CTA when the width is below 256, and few
 // lanes carry no row (a power-of-two width for the rest would leave up to
 // half of them empty).
-// same_groups: every tile of the bucket has the same splits per CTA -- the
-// dense sweep stages a CTA's columns in chunks shared by its groups, and the
-// power of two that a split's product drops depends on the chunk length, so
-// all rows of a split must see the same chunks.  Then a bucket of 256 rows or
-// more keeps full-width tiles to its end, and a smaller one is one tile.
+// same_groups: every tile of the bucket runs the same number of splits per
+// CTA -- the dense sweep stages a CTA's columns in chunks shared by its
+// groups, and the power of two that a split's product drops depends on the
+// chunk length, so all rows of a split must see the same chunks.  Then a
+// bucket of 256 * rpt rows or more keeps full tiles, one split per CTA, and
+// its last rows go in one tile of the rest's width that also runs one split
+// per CTA (groups = 1; the CTA's threads past it idle); a smaller bucket is
+// one tile.
 struct RowTile {
     uint32_t row0, tps;
     int rpt;
+    uint32_t groups = 0;     // splits per CTA; 0: 256 / tps
 };
+inline uint32_t group_width(uint32_t lanes, uint32_t min_tps) {
+    uint32_t t = min_tps;
+    if (lanes <= 32) { while (t < lanes) t <<= 1; }
+    else t = (lanes + 31) / 32 * 32;
+    return t;
+}
 inline void row_tiles(uint32_t n, int rpt, uint32_t min_tps, std::vector<RowTile>& out, bool same_groups = false) {
     out.clear();
     uint32_t r0 = 0;
     const uint32_t full = 256u * (uint32_t)rpt;
     while (n - r0 >= full) { out.push_back({ r0, 256u, rpt }); r0 += full; }
     if (same_groups && r0 > 0) {
-        if (n > r0) out.push_back({ r0, 256u, rpt });
+        const uint32_t rest = n - r0;
+        if (rest) out.push_back({ r0, group_width((rest + rpt - 1) / rpt, min_tps), rpt, 1u });
         return;
     }
     while (n - r0 >= 256u) { out.push_back({ r0, 256u, 1 }); r0 += 256u; }
     const uint32_t rest = n - r0;
     if (!rest) return;
-    if (same_groups && r0 > 0) { out.push_back({ r0, 256u, 1 }); return; }
-    uint32_t t = min_tps;
-    if (rest <= 32) { while (t < rest) t <<= 1; }
-    else t = (rest + 31) / 32 * 32;
-    out.push_back({ r0, t, 1 });
+    out.push_back({ r0, group_width(rest, min_tps), 1 });
 }
+// Splits one item of the tile runs.
+inline uint32_t tile_groups(const RowTile& t) { return t.groups ? t.groups : 256u / t.tps; }
 // The sweep items of one tile: one per split for full-width tiles, else one
-// per 256 / tps consecutive splits.
+// per tile_groups consecutive splits.
 template <class Push>
 inline void tile_items(const RowTile& t, uint32_t s_begin, uint32_t s_end, Push push) {
-    if (t.tps == 256) {
-        for (uint32_t s = s_begin; s < s_end; ++s) push(t.row0, s, 256u);
-    } else {
-        const uint32_t per = 256 / t.tps;
-        for (uint32_t s = s_begin; s < s_end; s += per) push(t.row0, s, t.tps);
-    }
+    const uint32_t per = tile_groups(t);
+    const uint32_t code = t.groups ? (t.tps | (t.groups << 16)) : t.tps;
+    for (uint32_t s = s_begin; s < s_end; s += per) push(t.row0, s, code);
 }
 
 // Limb width of residues mod p^2 for primes up to pmax_incl.

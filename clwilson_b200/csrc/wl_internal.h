@@ -80,9 +80,17 @@ inline void dense_shape(uint32_t nrows, int* rpt, uint32_t* tps) {
 
 // One CTA of the column sweep: threads [k*tps, (k+1)*tps) work on split
 // split0 + k; thread i of a group takes rows row0 + i + j*tps, j < RPT.
+// The CTA runs 256 / tps splits, except that a dense-sweep item may set its
+// count in the high half of `tps` (item_tps / item_groups): the last,
+// partly filled row tile of a bucket runs one split in a narrower group, with
+// the chunk length of the bucket's full tiles.
 struct SweepItem {
     uint32_t bucket, row0, split0, tps;
 };
+__host__ __device__ inline uint32_t item_tps(const SweepItem& it) { return it.tps & 0xFFFFu; }
+__host__ __device__ inline uint32_t item_groups(const SweepItem& it) {
+    return (it.tps >> 16) ? (it.tps >> 16) : 256u / (it.tps & 0xFFFFu);
+}
 
 // Per-row state beyond the modulus.
 struct RowInfo {

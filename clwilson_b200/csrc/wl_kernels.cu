@@ -522,15 +522,16 @@ k_sweep_dense(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ 
     static_assert(!SMB || (SORT && RPT == 1), "shared-memory buckets need the sorted kernel, one row per thread");
     const SweepItem it = items[blockIdx.x];
     const Bucket bk = buckets[it.bucket];
-    const uint32_t tps = it.tps;
-    const uint32_t G = 256 / tps;                 // splits in this CTA
-    if (G > DENSE_GMAX) return;                   // per-group tables hold DENSE_GMAX (host plans tps >= 8)
+    const uint32_t tps = item_tps(it);
+    const uint32_t G = item_groups(it);           // splits in this CTA
+    // per-group tables hold DENSE_GMAX groups (the host plans tps >= 8)
+    if (tps < 8 || tps > 256 || G == 0 || G > DENSE_GMAX || G * tps > 256) return;
     const uint32_t g = threadIdx.x / tps, lt = threadIdx.x % tps;
     const uint32_t KG = DENSE_CHUNK / G;          // staged columns per split and chunk
     const uint32_t s = it.split0 + g;
-    // lanes past the CTA's last whole group (tps need not divide 256) take no
-    // split; they still pass every barrier, and g == G < DENSE_GMAX keeps
-    // their per-group table rows in bounds
+    // threads past the CTA's last group (G * tps may be below 256) take no
+    // split; they still pass every barrier, and g = threadIdx.x / tps <= 31 <
+    // DENSE_GMAX keeps their per-group table rows in bounds
     const bool has_split = g < G && s < bk.ndense;
     const uint64_t T = bk.T;
 

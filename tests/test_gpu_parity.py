@@ -121,6 +121,20 @@ def test_capped_parity_with_oracle(engine, lo, hi):
         assert (int(got["s0"][i]), int(got["s1"][i])) == (int(want["s0"][i]), int(want["s1"][i])), int(got["p"][i])
 
 
+@pytest.mark.parametrize("lo,hi", [((1 << 62) - 1 - 60000, (1 << 62) - 1), (10**13, 10**13 + 60000)])
+def test_dense_partial_tiles_with_oracle(engine, lo, hi):
+    # Below 2^16 every column of these ranges is in the dense regime.  Their
+    # class buckets hold 256 to 1,000 rows: full 256-row tiles, then a last
+    # tile narrower than 256 lanes that runs one split per CTA, with the chunk
+    # length of the full tiles.  Every row against the oracle.
+    qcap = 1 << 16
+    got, _ = engine.rows(lo, hi, q_cap=qcap)
+    counts = [int((got["type"] == t).sum()) for t in range(3)]
+    assert all(c > 256 and c % 256 for c in counts), counts
+    want, _ = oracle.search(lo, hi, qcap=qcap)
+    _same_rows(got, want, fields=("p", "s0", "s1", "type"))
+
+
 def test_batch_matches_plain(engine):
     ranges = [(10**6, 10**6 + 5000), (10**8, 10**8 + 3000), (200, 564), (2**31 - 1000, 2**31 + 1000)]
     per, results, st = engine.batch(ranges)

@@ -45,18 +45,19 @@ uint64_t pi_upper_bound(uint64_t x) {   // Rosser-Schoenfeld: pi(x) < 1.25506 x 
 }  // namespace
 
 // Sweep kernel choices measured best on B200 (the digit-sorted dense kernel
-// with 3-bit windows, H every 8 columns; the wide-product cell, two rows per
+// with 3-bit windows and its buckets in shared memory, 4 CTAs per SM, H every
+// 8 columns; the wide-product cell, two rows per
 // thread for large buckets; CTA-per-row merges from 64 splits).  The
 // environment overrides them for experiments: WL_CELL_VARIANT, WL_DENSE_SORT,
 // WL_DENSE_CFG (42: 4-bit windows), WL_DENSE_HSTEP, WL_DENSE_KERNEL (a
 // WL_DENSE_* value); wl_autotune measures them.
 static void default_tuning(wl_ctx* c) {
     const char* e;
-    int kernel = DENSE_SORTED_W3, hstep = 8;
+    int kernel = DENSE_SMEM_W3, hstep = 8;
     const int sort = (e = getenv("WL_DENSE_SORT")) ? atoi(e) : 1;
     const int cfg = (e = getenv("WL_DENSE_CFG")) ? atoi(e) : 0;
     if ((e = getenv("WL_DENSE_HSTEP")) && atoi(e) > 0) hstep = atoi(e);
-    if (sort) kernel = cfg == 42 ? DENSE_SORTED_W4 : DENSE_SORTED_W3;
+    if (sort) kernel = cfg == 42 ? DENSE_SORTED_W4 : DENSE_SMEM_W3;
     const int forced = (e = getenv("WL_DENSE_KERNEL")) ? atoi(e) : -1;   // a WL_DENSE_* value
     for (int L = 2; L <= 4; ++L) {
         int k = kernel;
@@ -1219,9 +1220,9 @@ static int tune_on(wl_ctx* c, const wl_range* r, size_t nr, uint64_t qcap, uint3
         bool b;
         RC(trial(t, &b));
     }
-    const int dense_c[9][2] = { { DENSE_SORTED_W3, 4 }, { DENSE_SORTED_W3, 12 }, { DENSE_SORTED_W3, 16 },
-                                { DENSE_SORTED_W4, 8 }, { DENSE_SWITCH_W3, 8 }, { DENSE_SWITCH_W4, 8 },
-                                { DENSE_SMEM_W3, 8 }, { DENSE_SMEM_W4, 8 }, { DENSE_SORTED_W3_2CTA, 8 } };
+    const int dense_c[9][2] = { { DENSE_SMEM_W3, 4 }, { DENSE_SMEM_W3, 12 }, { DENSE_SMEM_W3, 16 },
+                                { DENSE_SORTED_W3, 8 }, { DENSE_SORTED_W4, 8 }, { DENSE_SWITCH_W3, 8 },
+                                { DENSE_SWITCH_W4, 8 }, { DENSE_SMEM_W4, 8 }, { DENSE_SORTED_W3_2CTA, 8 } };
     for (auto& dc : dense_c) {
         wl_tuning t = c->tune;
         apply([&](int i) { t.dense_kernel[i] = dc[0]; t.dense_hstep[i] = dc[1]; });

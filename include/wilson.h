@@ -227,11 +227,11 @@ int wl_column_product_noalloc(const uint64_t *primes, uint32_t nrows, uint64_t p
  * No counterpart in the reference.  The sweep kernels have variants whose
  * speed depends on the GPU and the workload; a context keeps one choice per
  * limb width L (index L - 2: p < 2^31, < 2^47, < 2^62). */
-#define WL_DENSE_SORTED_W3 0   /* digit-sorted windows, 3-bit, 3 CTAs/SM (default) */
+#define WL_DENSE_SORTED_W3 0   /* digit-sorted windows, 3-bit, 3 CTAs/SM */
 #define WL_DENSE_SORTED_W4 1   /* digit-sorted windows, 4-bit, 2 CTAs/SM */
 #define WL_DENSE_SWITCH_W3 2   /* per-column bucket switch, 3-bit, 3 CTAs/SM */
 #define WL_DENSE_SWITCH_W4 3   /* per-column bucket switch, 4-bit, 2 CTAs/SM */
-#define WL_DENSE_SMEM_W3   4   /* digit-sorted, buckets in shared memory, 3-bit, 4 CTAs/SM */
+#define WL_DENSE_SMEM_W3   4   /* digit-sorted, buckets in shared memory, 3-bit, 4 CTAs/SM (default) */
 #define WL_DENSE_SMEM_W4   5   /* digit-sorted, buckets in shared memory, 4-bit, 2 CTAs/SM */
 #define WL_DENSE_SORTED_W3_2CTA 6   /* digit-sorted windows, 3-bit, 2 CTAs/SM (no register spills) */
 typedef struct {

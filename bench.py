@@ -229,20 +229,29 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def host_threads() -> int:
+    """Host threads this process may run on.  The CPU legs pass it to the
+    oracle explicitly: torchrun sets OMP_NUM_THREADS=1 in every rank, which
+    would otherwise leave the reference arm on one thread at N > 1."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return max(1, os.cpu_count() or 1)
+
+
 def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
     """The oracle (reference algorithm restated in C, all host threads) on a
     bounded sample of rows of [lo, hi): primes per second."""
     import oracle
     oracle.build()
-    L = oracle.lib()
-    cores = int(L.orc_threads())
+    cores = host_threads()
     n = len(oracle.list_primes(lo, hi))
     k = max(1, cores)
     while True:
         step = max(1, n // k)
         sel = list(range(0, n, step))[:k]
         t0 = time.perf_counter()
-        rows, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        rows, targets = oracle.search(lo, hi, qcap=q_cap, threads=cores, rows=sel)
         dt = time.perf_counter() - t0
         if dt > budget_s / 3 or k >= n or k >= 512 * cores:
             break
@@ -268,7 +277,7 @@ def run_reference(args, rank, world):
     lo, hi = max(ranges, key=lambda r: r[1] - r[0])
     import oracle
     oracle.build()
-    cores = int(oracle.lib().orc_threads())
+    cores = host_threads()
     n = len(oracle.list_primes(lo, hi))
     # a step: `k` evenly spaced rows of the workload with all their columns,
     # k doubled from the core count until a step takes about 5 s, so that the
@@ -277,14 +286,14 @@ def run_reference(args, rank, world):
     while True:
         sel = list(range(0, n, max(1, n // k)))[:k]
         t0 = time.perf_counter()
-        _, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        _, targets = oracle.search(lo, hi, qcap=q_cap, threads=cores, rows=sel)
         if time.perf_counter() - t0 > 5.0 or k >= n or k >= 512 * cores:
             break
         k *= 2
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        rows, targets = oracle.search(lo, hi, qcap=q_cap, rows=sel)
+        rows, targets = oracle.search(lo, hi, qcap=q_cap, threads=cores, rows=sel)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)

@@ -138,6 +138,38 @@ __host__ __device__ __forceinline__ void cell_w(Res<L>& x, uint32_t q, const uin
     x.w[L - 1] = X[L - 1] + (uint32_t)(A >> 32);
 }
 
+// Step j of the Montgomery product of x by a multi-limb multiplier
+// W = sum_j w_j 2^(32j) (an exact product of several columns, shared by every
+// row): with x fixed and the accumulator t zero before the first step,
+//     t <- (t + x*w_j + m*n) / 2^32,   m = -(t + x*w_j) * n^-1 mod 2^32.
+// After the k limbs of W, t = x*W / 2^(32k) mod n.  With x < 2n and
+// t < x + n before a step, t + x*w_j + m*n < 2^32 (x + n), so t < x + n < 3n
+// after it: L limbs hold t while 3n < 2^(32L) (n = p^2 with p below 2^31,
+// 2^47, 2^62 for L = 2, 3, 4), and one conditional subtraction after the last
+// limb brings it below 2n.  The same 2L + 1 multiplies as a cell, for 32 bits
+// of multiplier instead of one column of 27 to 32 bits.
+template <int L>
+__host__ __device__ __forceinline__ void limb_step(uint32_t (&t)[L], const Res<L>& x, uint32_t w,
+                                                   const uint32_t* n, uint32_t ninv) {
+    uint64_t S = (uint64_t)x.w[0] * w + t[0];
+    const uint32_t u0 = (uint32_t)S;
+    uint32_t U[L];                                   // (t + x*w) >> 32, L limbs
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        S = (uint64_t)x.w[k] * w + t[k] + (S >> 32);
+        U[k - 1] = (uint32_t)S;
+    }
+    U[L - 1] = (uint32_t)(S >> 32);
+    const uint32_t m = u0 * ninv;
+    uint64_t A = (uint64_t)m * n[0] + u0;            // low word is zero
+#pragma unroll
+    for (int k = 1; k < L; ++k) {
+        A = (uint64_t)m * n[k] + U[k - 1] + (A >> 32);
+        t[k - 1] = (uint32_t)A;
+    }
+    t[L - 1] = U[L - 1] + (uint32_t)(A >> 32);
+}
+
 // As cell_w, with the first reduction product replaced by its high half:
 // lo(m*n0) = -t0 mod 2^32, so (m*n0 + t0) >> 32 = hi(m*n0) + (t0 != 0).
 __host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {

@@ -111,6 +111,14 @@ int ensure_columns(wl_ctx* c, uint64_t limit) {
     c->sieve_bytes += 2ull * nseg * SEG_WORDS * 4 + 2ull * nseg * 4 + 2ull * (nseg + 1) * 8 + total * 4;
     c->ncols = total;
     c->col_limit = nl;
+    // the exact products of the table's aligned column groups
+    c->ngroups = 0;
+    const uint64_t ng = total / COL_GROUP;
+    RC(ensure(c->gprod, (size_t)ng * COL_GROUP * 4 + 16));
+    RC(ensure(c->gk, (size_t)ng + 16));
+    launch_group_products(as<uint32_t>(c->cols), ng, as<uint32_t>(c->gprod), as<uint8_t>(c->gk), c->st);
+    c->launches++;
+    c->ngroups = ng;
     return 0;
 }
 
@@ -771,7 +779,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         else
             launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(c->buckets),
                          as<SweepItem>(c->items) + ioff, as<RowMod>(c->rowmod), as<uint32_t>(c->cols),
-                         as<uint4>(c->part), as<Deficit>(c->defs), c->st);
+                         as<uint4>(c->part), as<Deficit>(c->defs), c->st, col_groups(c));
         if (!g.items.empty()) c->launches++;
         ioff += g.items.size();
     }
@@ -1050,6 +1058,7 @@ void wl_drop_columns(wl_ctx* c) {
     if (!c) return;
     c->ncols = 0;
     c->col_limit = 0;
+    c->ngroups = 0;
 }
 
 int wl_search(wl_ctx* c, uint64_t pmin, uint64_t pmax, uint64_t q_cap, wl_result* results, size_t cap,

@@ -3,6 +3,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -131,6 +132,8 @@ struct wl_ctx {
     uint32_t nbase = 0;
     DevBuf cols;            // column cache: all primes < col_limit, ascending, u32
     uint64_t ncols = 0, col_limit = 0;
+    DevBuf gprod, gk;       // exact products of its aligned groups of COL_GROUP columns
+    uint64_t ngroups = 0;
     DevBuf bitmap, segcount, offsets;
     DevBuf tp, keys, counts, buckets, rowinfo, rowmod, items, part, ipart, defs, rowout, dsplit;
     // columns above 2^32
@@ -145,6 +148,18 @@ struct wl_ctx {
     uint64_t sieve_ints = 0, sieve_bytes = 0;
     DevBuf work;         // dense sweep work counters: column cells, window cells, products
 };
+
+// The column groups of the resident table for the prefix-fold sweep
+// (WL_COL_GROUPS=0 in the environment turns them off, for comparisons).
+inline wl::ColGroups col_groups(wl_ctx* c) {
+    static const bool off = getenv("WL_COL_GROUPS") && atoi(getenv("WL_COL_GROUPS")) == 0;
+    wl::ColGroups g;
+    if (off || !c->ngroups) return g;
+    g.gprod = as<uint32_t>(c->gprod);
+    g.gk = as<uint8_t>(c->gk);
+    g.ngroups = c->ngroups;
+    return g;
+}
 
 // A range's window of test primes and its classes.
 struct RangeState {

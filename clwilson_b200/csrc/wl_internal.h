@@ -140,8 +140,21 @@ void launch_compact_multi(uint32_t nseg, const uint64_t* seg_lo, const uint32_t*
 void launch_count_leq(const uint32_t* cols, uint64_t ncols, const uint64_t* keys, uint32_t nkeys,
                       uint64_t* out, cudaStream_t st);
 void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaStream_t st);
+// Column groups: the resident column table in aligned groups of COL_GROUP
+// primes, each group's exact product as little-endian 32-bit limbs
+// (gprod[COL_GROUP*g ..], gk[g] limbs, at most COL_GROUP).  ColGroups{} (no
+// table) makes the prefix-fold sweep take every column as one cell.
+constexpr uint32_t COL_GROUP = 32;
+struct ColGroups {
+    const uint32_t* gprod = nullptr;
+    const uint8_t* gk = nullptr;
+    uint64_t ngroups = 0;
+};
+void launch_group_products(const uint32_t* cols, uint64_t ngroups, uint32_t* gprod, uint8_t* gk, cudaStream_t st);
+// cols: the column table whose index 0 the groups are aligned to
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
-                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st);
+                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st,
+                  ColGroups groups = ColGroups());
 // dense sweep kernels: digit-sorted windows (3-bit at 3 CTAs/SM, 4-bit at
 // 2 CTAs/SM, 3-bit at 2 CTAs/SM with every value in registers), a per-column
 // bucket switch (3- and 4-bit), or digit-sorted windows with the buckets in

@@ -212,6 +212,32 @@ k_window_primes_multi(const WinDesc* __restrict__ d, uint32_t nr, uint32_t* __re
 // Count of columns <= key (binary search over the sorted column array).
 // ===========================================================================
 
+// Exact product of each aligned group of COL_GROUP resident columns (one
+// thread per group): little-endian 32-bit limbs gprod[COL_GROUP*g ..], gk[g]
+// of them with the top one nonzero.  Each prime adds at most one limb, so a
+// group takes at most COL_GROUP limbs.
+__global__ void __launch_bounds__(128) k_group_products(const uint32_t* __restrict__ cols, uint64_t ngroups,
+                                                        uint32_t* __restrict__ gprod, uint8_t* __restrict__ gk) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    uint32_t acc[COL_GROUP];
+    uint32_t len = 1;
+    acc[0] = 1;
+    const uint32_t* q = cols + g * COL_GROUP;
+    for (uint32_t i = 0; i < COL_GROUP; ++i) {
+        const uint32_t v = q[i];
+        uint32_t carry = 0;
+        for (uint32_t k = 0; k < len; ++k) {
+            const uint64_t x = (uint64_t)acc[k] * v + carry;
+            acc[k] = (uint32_t)x;
+            carry = (uint32_t)(x >> 32);
+        }
+        if (carry && len < COL_GROUP) acc[len++] = carry;
+    }
+    for (uint32_t k = 0; k < len; ++k) gprod[g * COL_GROUP + k] = acc[k];
+    gk[g] = (uint8_t)len;
+}
+
 __global__ void k_count_leq(const uint32_t* __restrict__ cols, uint64_t ncols, const uint64_t* __restrict__ keys,
                             uint32_t nkeys, uint64_t* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -321,7 +347,7 @@ __device__ __forceinline__ void cell_wide_r(int j, Res<L>& x, uint32_t q, const 
 template <int L, int RPT, int V>
 __global__ void __launch_bounds__(256)
 k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items, const RowMod* __restrict__ mods,
-        const uint32_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs) {
+        const uint32_t* __restrict__ cols, uint4* __restrict__ part, Deficit* __restrict__ defs, ColGroups grp) {
     const SweepItem it = items[blockIdx.x];
     if (threadIdx.x >= (256 / it.tps) * it.tps) return;   // lanes past the CTA's last whole group
     const Bucket bk = buckets[it.bucket];
@@ -361,6 +387,34 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
         const uint32_t* cp = cols + c0;
         const uint32_t* const ce = cols + c1;
         while (cp < ce) {
+            // a whole aligned group of columns with the current exponent: its
+            // exact product, limb by limb (gk limbs for COL_GROUP columns)
+            if (grp.gprod != nullptr && ((uint64_t)(cp - cols) & (COL_GROUP - 1)) == 0 && cp + COL_GROUP <= ce &&
+                (uint64_t)(cp - cols) / COL_GROUP < grp.ngroups && __ldg(cp + COL_GROUP - 1) <= thr) {
+                const uint64_t gi = (uint64_t)(cp - cols) / COL_GROUP;
+                const uint32_t k = grp.gk[gi];
+                const uint32_t* gw = grp.gprod + gi * COL_GROUP;
+                uint32_t t[RPT][L];
+#pragma unroll
+                for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                    for (int l = 0; l < L; ++l) t[j][l] = 0;
+#pragma unroll 4
+                for (uint32_t i = 0; i < k; ++i) {
+                    const uint32_t w = __ldg(gw + i);
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) limb_step<L>(t[j], P[j], w, n[j], ninv[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+#pragma unroll
+                    for (int l = 0; l < L; ++l) P[j].w[l] = t[j][l];
+                    cond_sub_chain(P[j], n[j]);
+                }
+                cp += COL_GROUP;
+                cells += k;
+                continue;
+            }
             if ((((uintptr_t)cp) & 31) == 0 && cp + 8 <= ce) {
                 const uint4 g0 = __ldg(reinterpret_cast<const uint4*>(cp));
                 const uint4 g1 = __ldg(reinterpret_cast<const uint4*>(cp) + 1);
@@ -1791,22 +1845,28 @@ void launch_setup_rows(const RowInfo* info, uint32_t nrows, RowMod* mods, cudaSt
     if (!nrows) return;
     k_setup_rows<<<(nrows + 255) / 256, 256, 0, st>>>(info, nrows, mods);
 }
+void launch_group_products(const uint32_t* cols, uint64_t ngroups, uint32_t* gprod, uint8_t* gk, cudaStream_t st) {
+    if (!ngroups) return;
+    k_group_products<<<(unsigned)((ngroups + 127) / 128), 128, 0, st>>>(cols, ngroups, gprod, gk);
+}
 template <int V>
 static void launch_sweep_v(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
-                           const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
-#define WL_SWEEP(LL, RR) k_sweep<LL, RR, V><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs)
+                           const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st,
+                           ColGroups g) {
+#define WL_SWEEP(LL, RR) k_sweep<LL, RR, V><<<nitems, 256, 0, st>>>(buckets, items, mods, cols, part, defs, g)
     if (L == 2) { if (rpt == 4) WL_SWEEP(2, 4); else if (rpt == 2) WL_SWEEP(2, 2); else WL_SWEEP(2, 1); }
     else if (L == 3) { if (rpt == 4) WL_SWEEP(3, 4); else if (rpt == 2) WL_SWEEP(3, 2); else WL_SWEEP(3, 1); }
     else { if (rpt == 4) WL_SWEEP(4, 4); else if (rpt == 2) WL_SWEEP(4, 2); else WL_SWEEP(4, 1); }
 #undef WL_SWEEP
 }
 void launch_sweep(int variant, int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
-                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st) {
+                  const RowMod* mods, const uint32_t* cols, uint4* part, Deficit* defs, cudaStream_t st,
+                  ColGroups g) {
     if (!nitems) return;
-    if (variant == 0) launch_sweep_v<0>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
-    else if (variant == 2) launch_sweep_v<2>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
-    else if (variant == 3) launch_sweep_v<3>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
-    else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st);
+    if (variant == 0) launch_sweep_v<0>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st, g);
+    else if (variant == 2) launch_sweep_v<2>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st, g);
+    else if (variant == 3) launch_sweep_v<3>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st, g);
+    else launch_sweep_v<1>(L, rpt, nitems, buckets, items, mods, cols, part, defs, st, g);
 }
 void launch_sweep_dense(int L, int rpt, uint32_t nitems, const Bucket* buckets, const SweepItem* items,
                         const RowMod* mods, const uint32_t* cols, const uint32_t* dsplit, uint4* part, Deficit* defs,

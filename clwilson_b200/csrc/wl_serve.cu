@@ -670,7 +670,7 @@ static int serve_step(wl_server* s) {
         else
             launch_sweep(c->tune.sparse_variant[g.L - 2], g.L, g.rpt, (uint32_t)g.items.size(), as<Bucket>(sl.sbuckets),
                          as<SweepItem>(sl.items) + ioff, as<RowMod>(s->mods), as<uint32_t>(c->cols),
-                         as<uint4>(sl.part), as<Deficit>(sl.defs), c->st);
+                         as<uint4>(sl.part), as<Deficit>(sl.defs), c->st, col_groups(c));
         s->ws.launches++;
         ioff += g.items.size();
     }

@@ -74,7 +74,8 @@ def test_set_tuning_rejects_bad_values(eng):
 
 def test_autotune_and_serving_with_tuning(eng):
     t = eng.autotune([(10**9, 10**9 + 100000)])
-    assert t["ms"][0] > 0 and t["sparse_variant"][0] in (0, 1, 2) and t["dense_kernel"][0] in range(7)
+    # any of the sparse cell formulations (0-3) may win on this box
+    assert t["ms"][0] > 0 and t["sparse_variant"][0] in (0, 1, 2, 3) and t["dense_kernel"][0] in range(7)
     assert eng.tuning == t
     t2 = eng.autotune(limbs=(4,))                      # built-in sample
     assert t2["ms"][2] > 0

@@ -282,9 +282,13 @@ __global__ void k_setup_rows(const RowInfo* __restrict__ info, uint32_t nrows, R
 // non-increasing, C = prod_{i: e_i > e_{i+1}} P_i^{e_i - e_{i+1}} (e_{c1} = 0).
 // Each prime therefore costs one cell; a fold A *= P^d happens only where the
 // exponent drops, which for q > sqrt(T) is once per distinct floor(T/q).
+// An aligned group of COL_GROUP columns with one exponent costs less: P is
+// multiplied by the group's exact product, one Montgomery limb step per 32
+// bits (limb_step), 27 to 29 steps for 32 primes of 27 to 29 bits.
 // Fold points depend on T only, so all rows of the bucket fold together.
-// Every cell drops a factor 2^32 and every full product 2^(32L); the total
-// ("deficit") is identical for all rows of a split and stored once per split.
+// Every cell or limb step drops a factor 2^32 and every full product
+// 2^(32L); the total ("deficit") is identical for all rows of a split and
+// stored once per split.
 // ===========================================================================
 
 __device__ __forceinline__ uint64_t legendre(uint64_t T, uint64_t q) {
@@ -501,19 +505,20 @@ k_sweep(const Bucket* __restrict__ buckets, const SweepItem* __restrict__ items,
 // so that prefix folding would pay an exponentiation per column.
 //
 // Each exponent is split as e = H*2^s + l with l < 2^s, s chosen per split so
-// that H changes about once per 64 columns:
+// that H changes about once per `hstep` columns (8 by default):
 //     prod q^e = (prod q^H)^(2^s) * prod q^l.
 // The first factor is the prefix-fold product on H (cheap folds, one cell per
 // column), raised to 2^s by s squarings.  The second is a windowed product
-// over 4-bit digits of l: for window j, column q goes into bucket
+// over DW-bit digits of l (3 or 4): for window j, column q goes into bucket
 // B[digit_j(l)] (one cell), and prod_d B_d^d is formed with two running
 // products.  Windows are combined from the top (Horner).  Cost: about
-// 1 + s/4 cells per column.
+// 1 + (s/DW)(1 - 2^-DW) cells per column, plus the folds and the per-split
+// combination products.
 //
 // The exponents are the same for every row of the bucket, so they are
 // computed once per CTA per chunk of columns into shared memory.  Each CTA
-// holds 256/tps splits (groups of tps threads), each group staging its own
-// chunk.  Deficits (powers of two dropped by Montgomery steps) are uniform per
+// holds item_groups(it) splits (groups of tps threads), each group staging
+// its own chunk.  Deficits (powers of two dropped by Montgomery steps) are uniform per
 // split and tracked exactly as in k_sweep.
 // ===========================================================================
 

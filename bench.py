@@ -518,6 +518,9 @@ def batched_record(eng, rank, world, dist, stream, flush, max_width, steps, plai
                    "l2": "256 MiB buffer written between steps", "columns": "re-sieved every step"},
         "e2e": {"value": cells_all / tot_wall, "unit": "mulmods/s"},
         "gpu_launches": sum(s.kernel_launches for s in stats),
+        "cuda_graph": {"nodes_per_step": sum(s.graph_nodes for s in stats) / steps,
+                       "host_ms_to_capture_end_and_instantiate": sum(s.ms_graph_build for s in stats) / steps,
+                       "note": "the sweep, merge, tail and lift launches of a wl_batch call as one CUDA graph"},
         "work": {"cell_equivalents_per_step": work_all / steps, "dense_share": dense_all / max(1.0, work_all),
                  "cell_equivalents_per_s_in_sweep": work_all / max(sweep_s, 1e-9),
                  "note": "every column cell, plus the dense sweep's window cells and its full products at "

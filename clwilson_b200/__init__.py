@@ -70,7 +70,8 @@ class _Stats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("ms_big", ctypes.c_double),
                 ("sieve_integers", ctypes.c_uint64), ("sieve_bytes", ctypes.c_uint64),
                 ("dense_column_cells", ctypes.c_uint64), ("dense_window_cells", ctypes.c_uint64),
-                ("dense_products", ctypes.c_uint64)]
+                ("dense_products", ctypes.c_uint64), ("graph_nodes", ctypes.c_uint64),
+                ("ms_graph_build", ctypes.c_double)]
 
 
 class _Tuning(ctypes.Structure):
@@ -247,13 +248,15 @@ class Stats:
     dense_column_cells: int = 0
     dense_window_cells: int = 0
     dense_products: int = 0
+    graph_nodes: int = 0
+    ms_graph_build: float = 0.0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.tested, tuple(s.per_class), tuple(s.targets), s.pi_maxtarget, s.cells, s.tail_steps,
                    s.checksum, s.results, s.kernel_launches, s.ms_device, s.ms_primes, s.ms_sieve, s.ms_sweep,
                    s.ms_iterate, s.ms_finish, s.h2d_bytes, s.d2h_bytes, s.ms_big, s.sieve_integers, s.sieve_bytes,
-                   s.dense_column_cells, s.dense_window_cells, s.dense_products)
+                   s.dense_column_cells, s.dense_window_cells, s.dense_products, s.graph_nodes, s.ms_graph_build)
 
 
 @dataclass

@@ -16,11 +16,15 @@
 //      (k_iterate), and the class lift + quotient (k_finish);
 //   5. results.txt lines (ascending p) and the checksum on the host
 //      (cl_wilson.cpp:872-900).
+// A batch (wl_batch) issues the device work of step 4 -- every sweep launch
+// of both streams, the merges, the tail and the lift -- as one CUDA graph,
+// captured from the two streams and launched once (ChainGraph).
 // Also here: searches in pieces (q_lo / init of run_ranges) and the
 // row-wise product of pieces (wl_rows_product), kernel tuning, and the C ABI;
 // serving sessions are in wl_serve.cu.
 #include <algorithm>
 #include <cerrno>
+#include <chrono>
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
@@ -139,6 +143,51 @@ struct RunOut {
     std::vector<uint64_t> range_row_off;  // rows of range r: [off[r], off[r+1])
     std::vector<uint64_t> range_targets;  // 3 per range
     uint64_t pi_maxtarget = 0, cells = 0, tail = 0;
+};
+
+// The device chain of a batch as one CUDA graph: stream capture of the main
+// stream (the dense sweep's stream joins it through the fork event and is
+// joined back), then one instantiation and one launch.  Early returns while
+// capturing end the capture (the partial graph is dropped); the graph and
+// its executable are destroyed with this object, which outlives the call's
+// final stream synchronisation.
+struct ChainGraph {
+    cudaStream_t capturing = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    size_t nodes = 0;
+    double ms_build = 0;   // host time of end of capture + instantiation
+    int begin(cudaStream_t st) {
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        capturing = st;
+        return 0;
+    }
+    // event records inside the capture become event-record nodes, so the
+    // phase timings still come from the graph's own run
+    cudaError_t record(cudaEvent_t e, cudaStream_t st) const {
+        return capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+    }
+    int launch() {
+        const auto t0 = std::chrono::steady_clock::now();
+        cudaStream_t st = capturing;
+        capturing = nullptr;
+        CK(cudaStreamEndCapture(st, &graph));
+        CK(cudaGraphGetNodes(graph, nullptr, &nodes));
+        CK(cudaGraphInstantiate(&exec, graph, 0));
+        ms_build = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        CK(cudaGraphLaunch(exec, st));
+        return 0;
+    }
+    ~ChainGraph() {
+        if (capturing) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(capturing, &g);
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();   // the call already returns its own error
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -404,7 +453,7 @@ int gen_test_primes(wl_ctx* c, const wl_range* ranges, size_t nr, std::vector<Ra
 // tail and the lift); init: the rows' running products before q_lo, two
 // digits (s0, s1) per row in output order, or NULL for 1.
 static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qcap, RunOut& out, wl_stats* st,
-                      uint64_t q_lo = 2, const uint64_t* init = nullptr) {
+                      uint64_t q_lo = 2, const uint64_t* init = nullptr, bool graph = false) {
     const bool full = (qcap == 0);
     c->launches = 0;
     c->h2d = c->d2h = 0;
@@ -743,6 +792,12 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     // per-row accumulators of the column products (1, or the resumed products)
     RC(ensure(c->uacc, (size_t)nrows * 16 + 16));
     RC(ensure(c->udef, db.size() * sizeof(Deficit) + 16));
+    RC(ensure(c->work, 24));
+    // from here to the lift the device work is fixed by the plan above: a
+    // batch issues it as one graph (no initial products to upload and no
+    // columns above 2^32, whose windows are planned from device counts)
+    ChainGraph cg;
+    if (graph && !init && !big_need) RC(cg.begin(c->st));
     launch_acc_init(nrows, (uint32_t)db.size(), as<uint4>(c->uacc), as<Deficit>(c->udef), c->st);
     c->launches++;
     if (init) {
@@ -759,10 +814,9 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
     }
     launch_setup_rows(as<RowInfo>(c->rowinfo), nrows, as<RowMod>(c->rowmod), c->st);
     c->launches++;
-    RC(ensure(c->work, 24));
     CK(cudaMemsetAsync(c->work.p, 0, 24, c->st));
     CK(cudaEventRecord(c->rows_ready, c->st));
-    cudaEventRecord(c->ev[2], c->st);
+    cg.record(c->ev[2], c->st);
     size_t ioff = 0;
     bool forked = false;
     for (auto& g : groups) {
@@ -814,7 +868,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         out.pi_maxtarget += pi_big;
         big = true;
     }
-    cudaEventRecord(c->ev[3], c->st);
+    cg.record(c->ev[3], c->st);
     // rows are ordered by limb width: one tail and one finish launch per width
     uint32_t rb = 0;
     std::vector<std::pair<int, std::pair<uint32_t, uint32_t>>> lgroups;   // L, [row begin, row end)
@@ -836,7 +890,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
             c->launches++;
         }
     }
-    cudaEventRecord(c->ev[4], c->st);
+    cg.record(c->ev[4], c->st);
     for (auto& g : lgroups) {
         launch_finish(g.first, as<Bucket>(c->buckets), as<RowInfo>(c->rowinfo), as<RowMod>(c->rowmod),
                       as<uint4>(c->part), as<Deficit>(c->defs), K, as<uint4>(c->ipart),
@@ -845,6 +899,7 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
                       big ? as<Deficit>(c->bdef) : nullptr);
         c->launches++;
     }
+    if (cg.capturing) RC(cg.launch());
     std::vector<RowOut> ro(nrows);
     CK(cudaMemcpyAsync(ro.data(), c->rowout.p, (size_t)nrows * sizeof(RowOut), cudaMemcpyDeviceToHost, c->st));
     c->d2h += (size_t)nrows * sizeof(RowOut);
@@ -884,13 +939,19 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         st->pi_maxtarget = out.pi_maxtarget;
         st->cells = out.cells;
         st->tail_steps = out.tail;
-        float a = 0;
-        cudaEventElapsedTime(&a, c->ev[0], c->ev[5]); st->ms_device = a;
-        cudaEventElapsedTime(&a, c->ev[0], c->ev[1]); st->ms_primes = a;
+        // -1 where a span cannot be timed (its error is not left pending)
+        auto span = [](cudaEvent_t e0, cudaEvent_t e1) -> double {
+            float a = 0;
+            if (cudaEventElapsedTime(&a, e0, e1) == cudaSuccess) return a;
+            (void)cudaGetLastError();
+            return -1.0;
+        };
+        st->ms_device = span(c->ev[0], c->ev[5]);
+        st->ms_primes = span(c->ev[0], c->ev[1]);
         st->ms_sieve = c->ms_sieve;
-        cudaEventElapsedTime(&a, c->ev[2], c->ev[3]); st->ms_sweep = a;
-        cudaEventElapsedTime(&a, c->ev[3], c->ev[4]); st->ms_iterate = a;
-        cudaEventElapsedTime(&a, c->ev[4], c->ev[5]); st->ms_finish = a;
+        st->ms_sweep = span(c->ev[2], c->ev[3]);
+        st->ms_iterate = span(c->ev[3], c->ev[4]);
+        st->ms_finish = span(c->ev[4], c->ev[5]);
         st->kernel_launches = c->launches;
         st->h2d_bytes = c->h2d;
         st->d2h_bytes = c->d2h;
@@ -900,6 +961,8 @@ static int run_ranges(wl_ctx* c, const wl_range* ranges, size_t nr, uint64_t qca
         st->dense_column_cells = dwork[0];
         st->dense_window_cells = dwork[1];
         st->dense_products = dwork[2];
+        st->graph_nodes = cg.nodes;
+        st->ms_graph_build = cg.ms_build;
     }
     return 0;
 }
@@ -1149,7 +1212,8 @@ int wl_batch(wl_ctx* c, const wl_range* ranges, size_t n, uint64_t q_cap, wl_ran
     if (!c || !ranges || n == 0) return WL_ERR_ARG;
     cudaSetDevice(c->device);
     RunOut ro;
-    RC(run_ranges(c, ranges, n, q_cap, ro, stats));
+    static const bool direct = getenv("WL_BATCH_GRAPH") && atoi(getenv("WL_BATCH_GRAPH")) == 0;
+    RC(run_ranges(c, ranges, n, q_cap, ro, stats, 2, nullptr, !direct));
     return summarize(ro, n, q_cap == 0, out, results, cap, nresults, stats);
 }
 

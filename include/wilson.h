@@ -122,6 +122,9 @@ typedef struct {
                                     exponent's low part, summed over rows */
     uint64_t dense_products;    /* full Montgomery products it executed, summed over rows (about
                                    L cells each) */
+    uint64_t graph_nodes;       /* nodes of the CUDA graph that carried the call's sweep, merges,
+                                   tail and lift (wl_batch); 0 when they were launched one by one */
+    double ms_graph_build;      /* host time to end that graph's capture and instantiate it */
 } wl_stats;
 
 /* Open a context on CUDA device `device`. */

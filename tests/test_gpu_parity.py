@@ -138,13 +138,18 @@ def test_dense_partial_tiles_with_oracle(engine, lo, hi):
 def test_batch_matches_plain(engine):
     ranges = [(10**6, 10**6 + 5000), (10**8, 10**8 + 3000), (200, 564), (2**31 - 1000, 2**31 + 1000)]
     per, results, st = engine.batch(ranges)
+    # the batch's sweep, merges, tail and lift ran as one CUDA graph (every
+    # class target is below 2^32); the per-range calls launch them one by one
+    assert st.graph_nodes > 0 and st.ms_sweep > 0
     for (lo, hi), pr in zip(ranges, per):
         one = engine.search(lo, hi)
+        assert one.stats.graph_nodes == 0
         assert pr["checksum"] == one.checksum
         assert pr["results"] == len(one.results)
     # capped
     ranges = [(10**13, 10**13 + 10000), (10**9, 10**9 + 10000), ((1 << 62) - 30000, (1 << 62) - 1)]
-    per, _, _ = engine.batch(ranges, q_cap=1 << 22)
+    per, _, st = engine.batch(ranges, q_cap=1 << 22)
+    assert st.graph_nodes > 0 and st.ms_sweep > 0
     for (lo, hi), pr in zip(ranges, per):
         rows, _ = engine.rows(lo, hi, q_cap=1 << 22)
         ck = int((rows["p"].astype(object) + rows["s0"].astype(object) + rows["s1"].astype(object)).sum()) % (1 << 64)

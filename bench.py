@@ -239,6 +239,10 @@ def host_threads() -> int:
         return max(1, os.cpu_count() or 1)
 
 
+CPU_COLUMNS = ("re-sieved every step in chunks of 2^24 integers; one thread sieves and builds the next chunk's "
+               "columns while the others multiply the rows by the current one")
+
+
 def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
     """The oracle (reference algorithm restated in C, all host threads) on a
     bounded sample of rows of [lo, hi): primes per second."""
@@ -256,18 +260,10 @@ def cpu_baseline(lo: int, hi: int, q_cap: int, budget_s: float = 20.0):
         if dt > budget_s / 3 or k >= n or k >= 512 * cores:
             break
         k *= 2
-    # the oracle sieves its columns on one thread in every call; time that part alone
-    limit = max(int(t) for t in targets) + 1
-    if q_cap:
-        limit = min(limit, q_cap)
-    t0 = time.perf_counter()
-    oracle.count_primes_below(limit)
-    sieve_s = time.perf_counter() - t0
     return {"value": len(sel) / dt, "unit": "primes/s", "cores": cores, "kind": "port",
             "sample": f"{len(sel)} of {n} primes of [{lo}, {hi}) evenly spaced, q_cap={q_cap}, "
                       f"{dt:.1f} s incl. the column sieve",
-            "sieve_share": sieve_s / dt,
-            "value_without_sieve": len(sel) / max(dt - sieve_s, 1e-9)}, rows, sel
+            "columns": CPU_COLUMNS}, rows, sel
 
 
 def run_reference(args, rank, world):
@@ -281,7 +277,7 @@ def run_reference(args, rank, world):
     n = len(oracle.list_primes(lo, hi))
     # a step: `k` evenly spaced rows of the workload with all their columns,
     # k doubled from the core count until a step takes about 5 s, so that the
-    # column sieve each step repeats does not dominate
+    # first column chunk, sieved before any row can start, does not dominate
     k = max(1, cores)
     while True:
         sel = list(range(0, n, max(1, n // k)))[:k]
@@ -298,13 +294,6 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
-    # the share of a step the oracle spends sieving its columns (one thread)
-    limit = max(int(t) for t in targets) + 1
-    if q_cap:
-        limit = min(limit, q_cap)
-    t0 = time.perf_counter()
-    oracle.count_primes_below(limit)
-    sieve_s = time.perf_counter() - t0
     if q_cap:
         # the capped sweep's unit: column cells (sieving primes q <= T, q < q_cap) of the sampled rows
         per_class = [oracle.count_primes_below(min(t, q_cap - 1) + 1) if t else 0 for t in targets]
@@ -321,7 +310,7 @@ def run_reference(args, rank, world):
         "config": {"workload": desc, "sample_rows_per_step": len(sel), "rows_in_workload": n},
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": f"{len(sel)} of {n} primes per step, evenly spaced, q_cap={q_cap}",
-                         "sieve_share": sieve_s / (tot / len(times))},
+                         "columns": CPU_COLUMNS},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -509,6 +509,15 @@ static column *build_columns(const u32 *primes, size_t np, u64 target, u64 qcap,
     return cols;
 }
 
+/* the columns of the sieve chunk [lo, min(lo + SIEVE_CHUNK, limit)) for the
+   three class targets */
+static void chunk_columns(const sieve_base *b, u64 lo, u64 limit, const u64 *targets, u64 qcap,
+                          uint8_t *scratch, u32 *buf, column **cols, size_t *ncol) {
+    const u64 hi = lo + SIEVE_CHUNK < limit ? lo + SIEVE_CHUNK : limit;
+    const size_t np = sieve_segment(b, lo, hi, scratch, buf);
+    for (int t = 0; t < 3; ++t) cols[t] = build_columns(buf, np, targets[t], qcap, &ncol[t]);
+}
+
 /* prime-power product of one column set into a residue (mulsmall.cl:32-58) */
 static u64x2 column_product(const tpconst *c, const column *cols, size_t ncol, u64x2 residue) {
     for (size_t j = 0; j < ncol; ++j) {
@@ -605,24 +614,38 @@ long orc_search(u64 pmin, u64 pmax, u64 qcap, int threads, const u32 *sel, size_
     if (threads > 0) omp_set_num_threads(threads);
 #endif
     /* the column sweep, chunk by chunk as the reference's main loop
-       (cl_wilson.cpp:1856-1929) */
+       (cl_wilson.cpp:1856-1929).  As there, the next chunk's columns are
+       prepared while the rows multiply the current one (the reference's host
+       sieves while its GPU works): one thread sieves and builds chunk k+1,
+       then joins the others on the rows of chunk k. */
     sieve_base base = make_base(slimit);
     uint8_t *scratch = (uint8_t *)malloc(SIEVE_CHUNK / 2 + 2);
     u32 *buf = (u32 *)malloc((SIEVE_CHUNK / 2 + 2) * sizeof(u32));
+    column *cols[2][3]; size_t ncol[2][3];
+    int cur = 0;
+    if (slimit > 0) chunk_columns(&base, 0, slimit, tt, qcap, scratch, buf, cols[0], ncol[0]);
     for (u64 lo = 0; lo < slimit; lo += SIEVE_CHUNK) {
-        u64 hi = lo + SIEVE_CHUNK < slimit ? lo + SIEVE_CHUNK : slimit;
-        size_t np = sieve_segment(&base, lo, hi, scratch, buf);
-        column *cols[3]; size_t ncol[3];
-        for (int t = 0; t < 3; ++t) cols[t] = build_columns(buf, np, tt[t], qcap, &ncol[t]);
+        const u64 nlo = lo + SIEVE_CHUNK;
+        const int nxt = cur ^ 1;
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel
 #endif
-        for (long i = 0; i < (long)nw; ++i) {
-            if (want && !want[i]) continue;
-            u32 t = types[i];
-            res[i] = column_product(&cs[i], cols[t], ncol[t], res[i]);
+        {
+#ifdef _OPENMP
+#pragma omp single nowait
+#endif
+            if (nlo < slimit) chunk_columns(&base, nlo, slimit, tt, qcap, scratch, buf, cols[nxt], ncol[nxt]);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1) nowait
+#endif
+            for (long i = 0; i < (long)nw; ++i) {
+                if (want && !want[i]) continue;
+                u32 t = types[i];
+                res[i] = column_product(&cs[i], cols[cur][t], ncol[cur][t], res[i]);
+            }
         }
-        for (int t = 0; t < 3; ++t) free(cols[t]);
+        for (int t = 0; t < 3; ++t) free(cols[cur][t]);
+        cur = nxt;
     }
     free(scratch); free(buf); free(base.p);
 

@@ -501,4 +501,19 @@ __device__ __forceinline__ uint64_t isqrt64(uint64_t n) {
     return x;
 }
 
+// Exponent of the prime q in T!: sum over k of floor(T / q^k) (Legendre's
+// formula; the reference's getPower, cl_wilson.cpp:1293-1313).  The terms come
+// as running quotients, floor(T / q^k) = floor(floor(T / q^(k-1)) / q), so a
+// term costs one division, and once a quotient and q fit 32 bits that division
+// is a 32-bit one (a 64-bit division costs several times as many multiplies).
+__host__ __device__ __forceinline__ uint64_t legendre(uint64_t T, uint64_t q) {
+    uint64_t t = T / q, e = 0;
+    while (t) {
+        e += t;
+        if (t < q) break;                           // the next term is zero
+        t = ((t | q) >> 32) == 0 ? (uint64_t)((uint32_t)t / (uint32_t)q) : t / q;
+    }
+    return e;
+}
+
 }  // namespace wl

@@ -291,16 +291,6 @@ __global__ void k_setup_rows(const RowInfo* __restrict__ info, uint32_t nrows, R
 // stored once per split.
 // ===========================================================================
 
-__device__ __forceinline__ uint64_t legendre(uint64_t T, uint64_t q) {
-    uint64_t e = 0, qq = q;
-    while (true) {
-        e += T / qq;
-        if (qq > T / q) break;
-        qq *= q;
-    }
-    return e;
-}
-
 template <int L>
 __device__ __forceinline__ void fold_pow(Res<L>& A, const Res<L>& P, uint64_t d, const uint32_t* n, uint32_t ninv) {
     Res<L> Y = P;
